@@ -1,0 +1,360 @@
+#!/usr/bin/env python3
+"""Benchmark of the fused lattice update on the D3Q19 sphere channel.
+
+Workload (one step = one time step of the whole lattice): D3Q19, 256x128x128,
+TRT (Lambda = 1/4) + Smagorinsky LES (Cs = 0.17) applied per node, tau0 = 0.52,
+sphere R = 12 at (64,64,64) with BFL curved links, Zou-He velocity inlet
+u = 0.05 and pressure outlet rho = 1, periodic y/z, in-kernel momentum
+exchange every step. FP32 populations; an FP16-storage leg runs the same
+workload. Seeded synthetic inputs (no dataset).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl wake|reference]
+
+N > 1 runs under torchrun: each rank advances its own replica (no data-path
+collective); timing is the max over ranks of the CUDA-event time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+BYTES_PER_NODE = {("d3q19", "f32"): 2 * 19 * 4 + 1, ("d3q19", "f16"): 2 * 19 * 2 + 1}
+FALLBACK_HBM_GBS = 6650.0
+WORKLOAD = ("D3Q19 TRT(Lambda=1/4)+Smagorinsky(Cs=0.17, applied) tau0=0.52, sphere R=12 at (64,64,64) with BFL "
+            "links, Zou-He inlet u=0.05 / outlet rho=1, periodic y/z, in-kernel momentum exchange, 256x128x128")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=4000)
+    p.add_argument("--warmup", type=int, default=50)
+    p.add_argument("--impl", choices=["wake", "reference"], default="wake")
+    p.add_argument("--no-fp16", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--graph", type=int, default=20, help="steps per captured CUDA graph (0: plain launches)")
+    return p.parse_args()
+
+
+def hbm_peak():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            return float(json.loads(f.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_launch(key):
+    f = ROOT / "profiles" / "traffic.json"
+    if f.exists():
+        try:
+            return json.loads(f.read_text()).get(key)
+        except Exception:
+            return None
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampler (200 ms) running across the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.samples = []
+        self.proc = None
+        self.gpu_id = gpu_id
+        self.window = (0.0, 0.0)
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.gpu_id:
+            cmd += ["-i", self.gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        threading.Thread(target=self._read, daemon=True).start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append((time.time(), [x.strip() for x in line.split(",")]))
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        t0, t1 = self.window
+        rows = [r for (t, r) in self.samples if t0 - 0.25 <= t <= t1 + 0.25] or [r for _, r in self.samples]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi samples"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[0]) for r in rows if num(r[0]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 4 + i and r[4 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": num(rows[0][1]),
+                "power_w_max": max((num(r[2]) or 0.0) for r in rows), "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def allmax(world, v):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def timed_steps(g, case, steps, warmup, world):
+    import torch
+
+    stream = torch.cuda.current_stream()
+    g.set_stream(stream.cuda_stream)
+    g.step(case.collision, use_les=case.les, smag_const=case.cs_smag, n=warmup)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    g.step(case.collision, use_les=case.les, smag_const=case.cs_smag, n=steps)
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    g.synchronize()
+    return allmax(world, start.elapsed_time(end))
+
+
+def reference_sample(case_ref, steps_cap, budget_s, threads=1):
+    """Time the reference's own LatticeGrid3D::step + momentum exchange (oracle/_ref) on host cores."""
+    import oracle
+
+    L = oracle.ref()
+    kind = "reference"
+    if L is None:
+        return None
+    c = case_ref
+    grids = []
+    for _ in range(threads):
+        gr = oracle.RefGrid3D(c.nx, c.ny, c.nz, c.tau)
+        gr.init_fields(c.rho, c.ux, c.uy, c.uz)
+        L.ref3d_set_periodic(gr._h, 1)
+        L.ref3d_set_solid_sphere(gr._h, *c.sphere)
+        L.ref3d_build_curved_sphere_links(gr._h, *c.sphere)
+        grids.append(gr)
+    # one warm-up step, then as many steps as fit in the budget
+    t0 = time.perf_counter()
+    grids[0].step_forces(1, c.collision, c.mem[:3], c.mem[3], use_les=True, cs=c.cs_smag)
+    t_step = time.perf_counter() - t0
+    n = int(max(1, min(steps_cap, budget_s // max(t_step, 1e-6))))
+
+    def run(gr):
+        gr.step_forces(n, c.collision, c.mem[:3], c.mem[3], use_les=True, cs=c.cs_smag)
+
+    ths = [threading.Thread(target=run, args=(gr,)) for gr in grids]
+    t0 = time.perf_counter()
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    dt = time.perf_counter() - t0
+    mlups = threads * c.n * n / dt / 1e6
+    return {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": kind,
+            "sample": f"{n} reference steps of the {c.nx}x{c.ny}x{c.nz} sphere channel (x-periodic, y/z walls, "
+                      f"TRT, LES flag on, BFL, momentum exchange per step){' x ' + str(threads) + ' replicas' if threads > 1 else ''}",
+            "seconds": dt, "steps": n}
+
+
+def run_reference_impl(args):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    from wake_b200 import workloads as W
+
+    c = W.sphere_channel(reference_variant=True, collision=1, les=False)
+    try:
+        import psutil
+
+        mem_cap = int(psutil.virtual_memory().available // (1.5 * 2**30))
+    except Exception:
+        mem_cap = 4
+    threads = max(1, min(os.cpu_count() or 1, 32, mem_cap))
+    res = reference_sample(c, steps_cap=max(1, args.steps), budget_s=90.0, threads=threads)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libwake_ref.so missing"}))
+        return
+    ms = res["seconds"] * 1e3 / res["steps"]
+    line = {"impl": "reference", "metric": "MLUPS", "value": res["value"], "unit": "MLUPS", "n_gpus": args.gpus,
+            "steps": res["steps"], "warmup": 1, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64)",
+            "config": {"workload": WORKLOAD + " [reference-expressible variant: x-periodic, y/z walls, no Zou-He, "
+                                                "LES computed but not applied]", "nodes": c.n},
+            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": res["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_impl(args)
+        return
+    world, rank, local = dist_setup(args)
+    import torch
+
+    import wake_b200 as wb
+    from wake_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    dev_uuid = None
+    try:
+        dev_uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    case = W.sphere_channel()
+    clocks = Clocks(dev_uuid)
+    clocks.start()
+    peak, peak_kind = hbm_peak()
+
+    # ---- FP32 leg (headline)
+    g = W.build_grid(case, storage="f32")
+    if args.graph:
+        g.use_graph(args.graph)
+    t_begin = time.time()
+    ms = timed_steps(g, case, args.steps, args.warmup, world)
+    clocks.window = (t_begin, time.time())
+    n_nodes = case.n
+    ms_step = ms / args.steps
+    value = world * n_nodes * args.steps / (ms * 1e-3) / 1e6
+    bpn = BYTES_PER_NODE[("d3q19", "f32")]
+    achieved = bpn * n_nodes / (ms_step * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": f"{peak_kind} HBM copy bandwidth", "traffic": traffic_per_launch("d3q19_f32_step"),
+            "bytes_per_node": bpn, "kernel": "wk::k_step<19, TRT, F32, LES>"}
+    forces = g.force_history()
+    del g
+    torch.cuda.empty_cache()
+
+    # ---- FP16-storage leg
+    fp16 = None
+    if not args.no_fp16:
+        g16 = W.build_grid(case, storage="f16")
+        if args.graph:
+            g16.use_graph(args.graph)
+        ms16 = timed_steps(g16, case, args.steps, args.warmup, world)
+        bpn16 = BYTES_PER_NODE[("d3q19", "f16")]
+        ach16 = bpn16 * n_nodes / (ms16 / args.steps * 1e-3) / 1e9
+        fp16 = {"value": world * n_nodes * args.steps / (ms16 * 1e-3) / 1e6, "unit": "MLUPS",
+                "ms_per_step": ms16 / args.steps, "speedup_vs_f32": ms / ms16,
+                "roofline": {"achieved": ach16, "peak": peak, "frac": ach16 / peak, "bytes_per_node": bpn16,
+                             "traffic": traffic_per_launch("d3q19_f16_step")}}
+        del g16
+        torch.cuda.empty_cache()
+
+    # ---- end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        g = W.build_grid(case, storage="f32")
+        if args.graph:
+            g.use_graph(args.graph)
+        f0_host = torch.from_numpy(g.f_src_data()).pin_memory()
+        out = {k: torch.empty(n_nodes, dtype=torch.float32).pin_memory() for k in ("rho", "ux", "uy", "uz", "speed")}
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        wb.check(wb.lib.wake_grid_set_populations(g.handle, f0_host.data_ptr()))
+        g.step(case.collision, use_les=case.les, smag_const=case.cs_smag, n=args.steps)
+        hist = g.force_history()
+        wb.check(wb.lib.wake_grid_get_macroscopic(g.handle, *[out[k].data_ptr() for k in ("rho", "ux", "uy", "uz",
+                                                                                         "speed")]))
+        dt = allmax(world, time.perf_counter() - t0)
+        h2d = f0_host.numel() * 4
+        d2h = hist.nbytes + sum(v.numel() * 4 for v in out.values())
+        e2e = {"value": world * n_nodes * args.steps / dt / 1e6, "unit": "MLUPS",
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "job": "H2D of the initial populations from pinned host memory, K fused steps through "
+                      "wake_grid_step, D2H of the per-step force history and of rho/u/speed"}
+        del g
+    clocks.stop()
+
+    # ---- CPU baseline (rank 0, N = 1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        c_ref = W.sphere_channel(reference_variant=True, collision=1, les=False)
+        res = reference_sample(c_ref, steps_cap=40, budget_s=20.0, threads=1)
+        if res is not None:
+            cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        cd = forces[-1, 0] / (0.5 * 0.05 ** 2 * math.pi * 144.0) if len(forces) else None
+        line = {"metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64; no dataset)",
+                "config": {"workload": WORKLOAD, "nodes": n_nodes, "storage": "f32",
+                           "l2": "inputs larger than L2 (two 319 MB population buffers, 126 MB L2)",
+                           "parallelism": "replicas" if world > 1 else "single GPU",
+                           "graph_steps": args.graph, "final_cd": cd},
+                "roofline": roof, "fp16": fp16, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
+                "gpu_launches": args.steps}
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

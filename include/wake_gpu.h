@@ -1,0 +1,248 @@
+/*
+ * wake_gpu.h - C ABI of the B200 lattice-update library (libwake_b200.so).
+ *
+ * Two layers:
+ *
+ * 1. Drop-in kernel entry points. Same symbol names, parameter lists and
+ *    meaning as the ISPC exports that the reference host declares in
+ *    `namespace ispc { extern "C" { ... } }` (src/grid/lattice_grid_2d.cpp:8-42,
+ *    src/grid/lattice_grid_3d.cpp:7-42, src/scenarios/karman_vortex.cpp:10-21,
+ *    src/scenarios/sphere_3d_wake.cpp:10-21, src/thermal/thermal_solver.cpp:6-44).
+ *    A build that links this library instead of the reference's
+ *    wake_ispc_kernels static library runs the reference host unchanged.
+ *    Pointers may be device memory (used in place) or ordinary host memory
+ *    (staged through the device). Each call is synchronous, like the
+ *    reference's, and returns void; failures are reported by
+ *    wake_gpu_last_error() (the reference has no error channel).
+ *    The ISPC `uniform float &` outputs of the momentum-exchange kernels are
+ *    plain pointers here (identical calling convention).
+ *
+ * 2. The fused engine (wake_grid_*): one resident lattice per handle,
+ *    advanced by one fused pull-stream + boundaries + moments +
+ *    momentum-exchange + collide kernel per step. This is the fast path a
+ *    GPU LatticeGrid2D/3D::step uses. Functions return 0 on success and a
+ *    negative WAKE_ERR_* code on failure (message in wake_gpu_last_error()).
+ */
+#ifndef WAKE_GPU_H
+#define WAKE_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ errors */
+#define WAKE_OK 0
+#define WAKE_ERR_INVALID (-1)   /* bad argument, size or state */
+#define WAKE_ERR_CUDA (-2)      /* CUDA runtime failure */
+#define WAKE_ERR_NOMEM (-3)     /* device allocation failed */
+#define WAKE_ERR_NUMERIC (-4)   /* non-finite or non-positive density seen on the device */
+
+/* Last error of the calling thread ("" if none); cleared by wake_gpu_clear_error. */
+const char* wake_gpu_last_error(void);
+int wake_gpu_last_error_code(void);
+void wake_gpu_clear_error(void);
+/* Library version string. */
+const char* wake_gpu_version(void);
+
+/* ------------------------------------------------- drop-in kernel entry points */
+/* D2Q9: src/ispc/d2q9_collision_bgk.ispc:5-16 */
+void d2q9_collide_bgk(const float f_in[], float f_out[], const uint8_t cell_type[], float rho[], float ux[],
+                      float uy[], float tau, float gx, float gy, int count);
+/* src/ispc/d2q9_collision_trt.ispc:7-19 */
+void d2q9_collide_trt(const float f_in[], float f_out[], const uint8_t cell_type[], float rho[], float ux[],
+                      float uy[], float tau_s, float tau_a, float gx, float gy, int count);
+/* src/ispc/d2q9_collision_mrt.ispc:6-18 */
+void d2q9_collide_mrt(const float f_in[], float f_out[], const uint8_t cell_type[], float rho[], float ux[],
+                      float uy[], float tau_shear, float tau_bulk, float gx, float gy, int count);
+/* src/ispc/d2q9_streaming.ispc:4-9 */
+void d2q9_stream_periodic(const float f_src[], float f_dst[], int nx, int ny);
+/* src/ispc/d2q9_streaming.ispc:33-41 */
+void d2q9_stream_with_boundaries(const float f_src[], float f_dst[], const uint8_t cell_type[], int nx, int ny,
+                                 float uw_x, float uw_y);
+/* src/ispc/d2q9_boundaries.ispc:5-11 */
+void d2q9_apply_bounce_back(float f[], const uint8_t cell_type[], float uw_x, float uw_y, int count);
+/* src/ispc/d2q9_boundaries.ispc:43-52 */
+void d2q9_apply_zou_he_inflow_west(float f[], float rho[], float ux[], float uy[], float u_in_x, float u_in_y,
+                                   int nx, int ny);
+/* src/ispc/d2q9_boundaries.ispc:85-93 */
+void d2q9_apply_zou_he_outflow_east(float f[], float rho[], float ux[], float uy[], float rho_out, int nx, int ny);
+/* src/ispc/d2q9_boundaries.ispc:125-131 */
+void d2q9_apply_convective_outflow_east(float f[], const float f_prev[], float u_conv, int nx, int ny);
+/* src/ispc/d2q9_les.ispc:6-15 */
+void d2q9_compute_smagorinsky_tau(const float f[], const float rho[], const float ux[], const float uy[],
+                                  float tau_eff[], float tau_0, float smagorinsky_constant, int count);
+/* src/ispc/d2q9_moments.ispc:4-10, 35-43, 68-73 */
+void d2q9_compute_macroscopic_moments(const float f[], float rho[], float ux[], float uy[], int count);
+void d2q9_compute_macroscopic_moments_forced(const float f[], float rho[], float ux[], float uy[], float gx,
+                                             float gy, int count);
+void d2q9_compute_velocity_magnitude(const float ux[], const float uy[], float speed[], int count);
+/* src/ispc/forces_momentum_exchange.ispc:6-18 (uniform float & -> float *) */
+void d2q9_compute_momentum_exchange_forces(const float f_post_collision[], const uint8_t cell_type[], int nx,
+                                           int ny, float center_x, float center_y, float max_radius,
+                                           float* fx_out, float* fy_out, float* torque_z_out);
+
+/* D3Q19: src/ispc/d3q19_collision_bgk.ispc:4-17, d3q19_collision_trt.ispc:5-19, d3q19_collision_mrt.ispc:26-40 */
+void d3q19_collide_bgk(const float f_in[], float f_out[], const uint8_t cell_type[], float rho[], float ux[],
+                       float uy[], float uz[], float tau, float gx, float gy, float gz, int count);
+void d3q19_collide_trt(const float f_in[], float f_out[], const uint8_t cell_type[], float rho[], float ux[],
+                       float uy[], float uz[], float tau_s, float tau_a, float gx, float gy, float gz, int count);
+void d3q19_collide_mrt(const float f_in[], float f_out[], const uint8_t cell_type[], float rho[], float ux[],
+                       float uy[], float uz[], float tau_shear, float tau_bulk, float gx, float gy, float gz,
+                       int count);
+/* src/ispc/d3q19_streaming.ispc:4-10, 39-49 */
+void d3q19_stream_periodic(const float f_src[], float f_dst[], int nx, int ny, int nz);
+void d3q19_stream_with_boundaries(const float f_src[], float f_dst[], const uint8_t cell_type[], int nx, int ny,
+                                  int nz, float uw_x, float uw_y, float uw_z);
+/* src/ispc/d3q19_curved.ispc:7-20 */
+void d3q19_apply_curved_bfl(float f_dst[], const float f_src[], const int fluid_indices[], const int q_dirs[],
+                            const float delta_fractions[], const float uw_x[], const float uw_y[],
+                            const float uw_z[], int nx, int ny, int nz, int num_boundary_links);
+/* src/ispc/d3q19_les.ispc:7-17 */
+void d3q19_compute_smagorinsky_tau(const float f[], const float rho[], const float ux[], const float uy[],
+                                   const float uz[], float tau_eff[], float tau_0, float smagorinsky_constant,
+                                   int count);
+/* src/ispc/d3q19_moments.ispc:4-11, 35-45, 69-75 */
+void d3q19_compute_macroscopic_moments(const float f[], float rho[], float ux[], float uy[], float uz[], int count);
+void d3q19_compute_macroscopic_moments_forced(const float f[], float rho[], float ux[], float uy[], float uz[],
+                                              float gx, float gy, float gz, int count);
+void d3q19_compute_velocity_magnitude(const float ux[], const float uy[], const float uz[], float speed[],
+                                      int count);
+/* src/ispc/forces_momentum_exchange.ispc:71-84 */
+void d3q19_compute_momentum_exchange_forces(const float f_post_collision[], const uint8_t cell_type[], int nx,
+                                            int ny, int nz, float center_x, float center_y, float center_z,
+                                            float max_radius, float* fx_out, float* fy_out, float* fz_out);
+
+/* D3Q27: src/ispc/d3q27_collision_mrt.ispc:5-18 (TRT), d3q27_moments.ispc:4-11, d3q27_streaming.ispc:4-10 */
+void d3q27_collide(const float f_in[], float f_out[], const uint8_t cell_type[], float rho[], float ux[],
+                   float uy[], float uz[], float tau_s, float tau_a, float gx, float gy, float gz, int count);
+void d3q27_compute_macroscopic_moments(const float f[], float rho[], float ux[], float uy[], float uz[], int count);
+void d3q27_stream_periodic(const float f_src[], float f_dst[], int nx, int ny, int nz);
+
+/* Thermal D2Q9: src/ispc/thermal_kernels.ispc:4-13, 48-55, 63-69 */
+void thermal_collide_d2q9(const float g_in[], float g_out[], const uint8_t cell_type[], const float ux[],
+                          const float uy[], float temperature[], float tau_T, int count);
+void thermal_compute_buoyancy_force_2d(const float temperature[], float gy_body[], float t_ref, float beta,
+                                       float g_gravity, int count);
+void thermal_apply_isothermal_wall(float g[], int nx, int ny, int y_wall, float t_wall);
+
+/* ---------------------------------------------------------- fused engine */
+typedef struct wake_grid wake_grid;
+
+/* Storage of the resident populations. */
+#define WAKE_STORE_F32 0
+#define WAKE_STORE_F16 1   /* FP16 of f_q / w_q - 1 */
+#define WAKE_STORE_BF16 2  /* BF16 of f_q / w_q - 1 */
+
+/* Collision models (values of the reference's CollisionType, include/wake/core/types.hpp:80-85). */
+#define WAKE_BGK 0
+#define WAKE_TRT 1
+#define WAKE_MRT 2
+
+/* Cell types (include/wake/core/types.hpp:69-77). */
+#define WAKE_CELL_FLUID 0
+#define WAKE_CELL_SOLID 1
+#define WAKE_CELL_INFLOW 2
+#define WAKE_CELL_OUTFLOW 3
+#define WAKE_CELL_MOVING_WALL 6
+
+/* q = 9 (nz must be 1), 19 or 27. Like LatticeGrid2D/3D's constructors
+ * (lattice_grid_2d.cpp:46-62, lattice_grid_3d.cpp:46-64) the lattice starts at
+ * rest with rho = 1 and every cell Fluid. Returns NULL on failure. */
+wake_grid* wake_grid_create(int q, int nx, int ny, int nz, float tau, int storage);
+void wake_grid_destroy(wake_grid* g);
+
+/* Work on this CUDA stream (cudaStream_t passed as void*); NULL = library stream. */
+int wake_grid_set_stream(wake_grid* g, void* stream);
+
+/* Collision model. les = 1 applies the Smagorinsky tau per node (the reference
+ * computes it but never feeds it to the collision, lattice_grid_2d.cpp:205).
+ * lambda_trt: TRT magic parameter (reference 0.25). tau_bulk: MRT bulk rate
+ * (reference 1.63 in 2D, 1.19 in 3D). mrt_exact: D3Q19 only, 0 = the
+ * reference's 7-digit inverse table, 1 = exact inverse. s3, s4: D3Q27 MRT
+ * third- and higher-order rates. */
+int wake_grid_set_model(wake_grid* g, int collision, int les, float cs_smag, float lambda_trt, float tau_bulk,
+                        int mrt_exact, float s3, float s4);
+int wake_grid_set_relaxation_time(wake_grid* g, float tau);
+
+/* Geometry (lattice_grid_2d.cpp:122-184, lattice_grid_3d.cpp:133-215). */
+int wake_grid_set_cell_type(wake_grid* g, int x, int y, int z, int type);
+int wake_grid_set_cell_types(wake_grid* g, const uint8_t* types /* host [nx*ny*nz] */);
+int wake_grid_get_cell_types(wake_grid* g, uint8_t* types /* host [nx*ny*nz] */);
+int wake_grid_set_solid_box(wake_grid* g, int x0, int y0, int z0, int x1, int y1, int z1);
+int wake_grid_set_solid_circle(wake_grid* g, float cx, float cy, float radius);
+int wake_grid_set_solid_sphere(wake_grid* g, float cx, float cy, float cz, float radius);
+/* Velocity inlet (Zou-He) on x = 0 and pressure outlet on x = nx-1. 2D follows
+ * the reference exactly (rows 1..ny-2, d2q9_boundaries.ispc:56,98); 3D applies
+ * the D3Q19 on-site scheme on Inflow / Outflow cells of those faces. */
+int wake_grid_set_inflow_west(wake_grid* g, float ux, float uy, float uz);
+int wake_grid_set_outflow_east(wake_grid* g, float rho_out);
+/* Moving lid: 2D north row (set_moving_wall_north), 3D top y = ny-1 plane. */
+int wake_grid_set_moving_wall(wake_grid* g, float uw_x, float uw_y, float uw_z);
+/* 3D: wrap y / z instead of half-way bounce-back walls. */
+int wake_grid_set_periodic(wake_grid* g, int periodic_y, int periodic_z);
+/* BFL curved links (arrays in host memory; uw may be NULL for resting walls). */
+int wake_grid_set_curved_links(wake_grid* g, int n, const int* fluid_indices, const int* q_dirs,
+                               const float* delta, const float* uw_x, const float* uw_y, const float* uw_z);
+/* Link builder of LatticeGrid3D::build_curved_sphere_links (lattice_grid_3d.cpp:217-290). */
+int wake_grid_build_curved_sphere_links(wake_grid* g, float cx, float cy, float cz, float radius);
+int wake_grid_num_curved_links(wake_grid* g);
+int wake_grid_get_curved_links(wake_grid* g, int* fluid_indices, int* q_dirs, float* delta);
+
+/* Initial state: equilibrium of uniform / per-node fields (initialize,
+ * initialize_custom), or raw populations f_src [q][node] in host memory. */
+int wake_grid_initialize(wake_grid* g, float rho, float ux, float uy, float uz);
+int wake_grid_initialize_fields(wake_grid* g, const float* rho, const float* ux, const float* uy, const float* uz);
+int wake_grid_set_populations(wake_grid* g, const float* f /* host [q][nx*ny*nz] */);
+/* Same, from device memory (no host staging). */
+int wake_grid_set_populations_device(wake_grid* g, const float* f_dev /* device [q][nx*ny*nz] */);
+
+/* Momentum-exchange monitor (forces_momentum_exchange.ispc:6-138): one force
+ * record per step, (Fx, Fy, Tz) in 2D and (Fx, Fy, Fz) in 3D, summed in FP64
+ * in a fixed order. history_capacity records are kept (ring). */
+int wake_grid_enable_forces(wake_grid* g, float cx, float cy, float cz, float r_max, int history_capacity);
+int wake_grid_disable_forces(wake_grid* g);
+/* Copies up to max records, oldest first, of the last min(steps, capacity)
+ * steps; returns the number copied or a negative error. */
+int wake_grid_get_force_history(wake_grid* g, double* out /* [max][3] */, int max);
+/* Number of steps recorded since forces were enabled. */
+long long wake_grid_force_count(wake_grid* g);
+
+/* Advance n steps with body force (gx, gy, gz). */
+int wake_grid_step(wake_grid* g, int n, float gx, float gy, float gz);
+/* Capture n steps in a CUDA graph (replayed by wake_grid_step whenever n is a
+ * multiple of the captured count and nothing was reconfigured). 0 disables. */
+int wake_grid_use_graph(wake_grid* g, int steps_per_graph);
+long long wake_grid_step_count(wake_grid* g);
+/* Block until the grid's stream is idle; reports device-side numeric errors. */
+int wake_grid_synchronize(wake_grid* g);
+
+/* Reference-visible state after the last step: f_src [q][node], and
+ * rho/ux/uy/uz/speed (moments_forced + velocity magnitude). Host or device
+ * pointers; uz may be NULL in 2D. */
+int wake_grid_get_populations(wake_grid* g, float* f);
+int wake_grid_get_macroscopic(wake_grid* g, float* rho, float* ux, float* uy, float* uz, float* speed);
+/* Diagnostics over Fluid cells (lattice_grid_2d.cpp:267-295), summed in FP64. */
+int wake_grid_diagnostics(wake_grid* g, double* total_mass, double* kinetic_energy, double* max_speed);
+/* Mass over every non-solid cell, FP64 (global conservation check). */
+int wake_grid_total_mass(wake_grid* g, double* mass);
+
+/* Introspection for benchmarks and tests. */
+int wake_grid_info(wake_grid* g, int* q, int* nx, int* ny, int* nz, int* storage, long long* pitch);
+/* Device pointer of the state buffer holding g^k (which = 0) or the other one (which = 1). */
+void* wake_grid_state_buffer(wake_grid* g, int which);
+/* Launch shape of the fused kernel: threads per block (32..512, multiple of 32). */
+int wake_grid_set_block(wake_grid* g, int threads_per_block);
+int wake_grid_get_block(wake_grid* g);
+
+/* FP64 Strouhal frequency of a lift history (strouhal_analyzer.cpp:39-84:
+ * mean removed, Hann window over the first min(n, 4096) samples, radix-2 FFT,
+ * peak bin >= 1). Returns the frequency; St = f D / U. */
+double wake_strouhal_frequency(const double* signal, int n, double dt);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WAKE_GPU_H */

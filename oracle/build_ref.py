@@ -1,0 +1,91 @@
+#!/usr/bin/env python3
+"""Build recipe for the reference's own CPU lattice-update path (test infrastructure only).
+
+The reference (Aneesh495/wake) compiles its kernels with the ISPC compiler
+(src/ispc/CMakeLists.txt:1-36, target avx2-i32x8, --opt=fast-math). ISPC is not
+installed in this image, so the kernel sources are translated mechanically into
+C++ at build time:
+
+  * ``foreach (i = a ... b)``   -> ``for (int i = a; i < b; ++i)``
+  * ``export``                  -> ``extern "C"``
+  * ``uniform`` / ``varying``   -> dropped (one lane per loop iteration)
+  * ``uint8``                   -> ``uint8_t``;  ``reduce_add(x)`` -> ``x``
+
+Nothing else is changed: every arithmetic expression is the reference's own.
+The translated files are written to ``oracle/_ref/gen`` and compiled with g++
+(-O3 -march=x86-64-v3 -ffast-math, mirroring ISPC's avx2 fast-math build)
+together with the reference's host C++ compiled from where it lies
+(src/grid/lattice_grid_2d.cpp, src/grid/lattice_grid_3d.cpp, src/core/memory.cpp)
+and the thin extern "C" shim ``oracle/ref_shim.cpp``. The output is
+``oracle/_ref/libwake_ref.so``. Nothing is copied into the repository: the
+output directory is git-ignored.
+
+Only tests, the smoke check and bench.py's reference arm use the result.
+"""
+from __future__ import annotations
+
+import os
+import re
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+OUT = HERE / "_ref"
+GEN = OUT / "gen"
+
+PRELUDE_H = """#pragma once
+#include <cmath>
+#include <cstdint>
+#include <algorithm>
+using std::sqrt; using std::min; using std::max; using std::floor; using std::abs; using std::cos;
+typedef uint8_t uint8;
+static inline float reduce_add(float v) { return v; }
+"""
+PRELUDE = '// Mechanically translated from ISPC by oracle/build_ref.py. Do not edit.\n#include "ispc_prelude.h"\n'
+
+
+FOREACH = re.compile(r"foreach\s*\(\s*(\w+)\s*=\s*(.+?)\s*\.\.\.\s*(.+?)\s*\)\s*\{")
+
+
+def reference_dir() -> Path:
+    return Path(os.environ.get("WAKE_REFERENCE_DIR", "/root/reference"))
+
+
+def translate(text: str) -> str:
+    text = FOREACH.sub(lambda m: f"for (int {m.group(1)} = {m.group(2)}; {m.group(1)} < {m.group(3)}; ++{m.group(1)}) {{", text)
+    text = re.sub(r"\bexport\s+void\b", 'extern "C" void', text)
+    text = re.sub(r"\b(uniform|varying)\b\s*", "", text)
+    return text
+
+
+def build(verbose: bool = False) -> Path:
+    ref = reference_dir()
+    if not (ref / "src" / "ispc").is_dir():
+        raise FileNotFoundError(f"reference sources not found under {ref}")
+    (GEN / "include" / "wake" / "ispc").mkdir(parents=True, exist_ok=True)
+    (GEN / "include" / "ispc_prelude.h").write_text(PRELUDE_H)
+    for isph in sorted((ref / "include" / "wake" / "ispc").glob("*.isph")):
+        body = translate(isph.read_text())
+        (GEN / "include" / "wake" / "ispc" / isph.name).write_text(PRELUDE + body)
+    cpp_files = []
+    for ispc in sorted((ref / "src" / "ispc").glob("*.ispc")):
+        dst = GEN / (ispc.stem + ".cpp")
+        dst.write_text(PRELUDE + translate(ispc.read_text()))
+        cpp_files.append(str(dst))
+    host = [ref / "src" / "grid" / "lattice_grid_2d.cpp",
+            ref / "src" / "grid" / "lattice_grid_3d.cpp",
+            ref / "src" / "core" / "memory.cpp",
+            ref / "src" / "forces" / "strouhal_analyzer.cpp"]
+    so = OUT / "libwake_ref.so"
+    cmd = ["g++", "-std=c++20", "-O3", "-march=x86-64-v3", "-ffast-math", "-fPIC", "-shared",
+           f"-I{GEN / 'include'}", f"-I{ref / 'include'}",
+           *cpp_files, *map(str, host), str(HERE / "ref_shim.cpp"), "-o", str(so)]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return so
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

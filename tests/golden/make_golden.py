@@ -1,0 +1,293 @@
+#!/usr/bin/env python3
+"""Generate the golden fixtures in this directory from the reference itself.
+
+Runs the reference's own host classes and its ISPC kernels (mechanically
+translated to C++ by oracle/build_ref.py, as ISPC is not installed here) on
+small seeded inputs and stores inputs and outputs as .npz files. The GPU tests
+compare against these files, so they need neither the reference sources nor
+its build on the GPU machine.
+
+    python tests/golden/make_golden.py     (needs the reference sources)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+import oracle  # noqa: E402
+from wake_b200 import workloads as W  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+
+
+def a(x):
+    return None if x is None else x.ctypes.data
+
+
+def save(name, **arrays):
+    np.savez_compressed(OUT / f"{name}.npz", **arrays)
+    print(f"wrote {name}.npz ({(OUT / f'{name}.npz').stat().st_size} bytes)")
+
+
+def cylinder_cases(R):
+    for coll, tag in ((0, "bgk"), (1, "trt"), (2, "mrt")):
+        c = W.cylinder_channel(nx=64, ny=32, diameter=8, cx=16, cy=16, tau=0.56, collision=coll)
+        g = oracle.RefGrid2D(c.nx, c.ny, c.tau)
+        g.init_fields(c.rho, c.ux, c.uy)
+        R.ref2d_set_inflow_west(g._h, 0.05, 0.0)
+        R.ref2d_set_outflow_east(g._h, 1.0)
+        for x in range(c.nx):
+            R.ref2d_set_cell_type(g._h, x, 0, 1)
+            R.ref2d_set_cell_type(g._h, x, c.ny - 1, 1)
+        R.ref2d_set_solid_circle(g._h, 16.0, 16.0, 4.0)
+        assert (g.cell_types() == c.types).all()
+        f0 = g.f()
+        hist = g.step_forces(200, coll, 16.0, 16.0, 12.0)
+        m = g.macro()
+        save(f"cyl2d_{tag}", f0=f0, types=c.types, steps=np.int32(200), tau=np.float32(c.tau), collision=np.int32(coll),
+             rho=m["rho"], ux=m["ux"], uy=m["uy"], speed=m["speed"], forces=hist, f_end=g.f())
+
+
+def cavity_case(R):
+    n = 32
+    g = oracle.RefGrid2D(n, n, 0.6)
+    g.init_fields(np.ones(n * n, np.float32), np.zeros(n * n, np.float32), np.zeros(n * n, np.float32))
+    for x in range(n):
+        R.ref2d_set_cell_type(g._h, x, 0, 1)
+    for y in range(n):
+        R.ref2d_set_cell_type(g._h, 0, y, 1)
+        R.ref2d_set_cell_type(g._h, n - 1, y, 1)
+    R.ref2d_set_moving_wall_north(g._h, 0.1)
+    f0 = g.f()
+    # the reference's lid row is itself collided and streamed as fluid and pulls the wall
+    # momentum from its lid neighbours; the cavity diverges after ~120 steps, so stop at 80
+    g.step(80, 2)
+    m = g.macro()
+    save("cavity2d_mrt", f0=f0, types=g.cell_types(), steps=np.int32(80), tau=np.float32(0.6), lid=np.float32(0.1),
+         rho=m["rho"], ux=m["ux"], uy=m["uy"])
+
+
+def poiseuille_case(R):
+    # body-force channel (tests/validation/test_poiseuille_convergence.cpp:12-31), TRT
+    nx, ny = 8, 33
+    g = oracle.RefGrid2D(nx, ny, 0.8)
+    for x in range(nx):
+        R.ref2d_set_cell_type(g._h, x, 0, 1)
+        R.ref2d_set_cell_type(g._h, x, ny - 1, 1)
+    f0 = g.f()
+    g.step(500, 1, 1e-4, 0.0)
+    m = g.macro()
+    save("poiseuille2d_trt", f0=f0, types=g.cell_types(), steps=np.int32(500), tau=np.float32(0.8), gx=np.float32(1e-4),
+         rho=m["rho"], ux=m["ux"], uy=m["uy"])
+
+
+def sphere_cases(R):
+    for coll, tag in ((0, "bgk"), (1, "trt"), (2, "mrt")):
+        c = W.sphere_channel(nx=24, ny=16, nz=16, radius=4.0, center=(8.0, 8.0, 8.0), tau=0.6, collision=coll,
+                             reference_variant=True)
+        g = oracle.RefGrid3D(c.nx, c.ny, c.nz, c.tau)
+        g.init_fields(c.rho, c.ux, c.uy, c.uz)
+        R.ref3d_set_periodic(g._h, 1)
+        R.ref3d_set_solid_sphere(g._h, 8.0, 8.0, 8.0, 4.0)
+        R.ref3d_build_curved_sphere_links(g._h, 8.0, 8.0, 8.0, 4.0)
+        assert (g.cell_types() == c.types).all()
+        idx, q, d = g.links()
+        f0 = g.f()
+        hist = g.step_forces(60, coll, (8.0, 8.0, 8.0), 8.0)
+        m = g.macro()
+        save(f"sphere3d_{tag}", f0_node=f0[:, 0].copy(), types=c.types, links_idx=idx, links_q=q, links_delta=d,
+             steps=np.int32(60), tau=np.float32(c.tau), collision=np.int32(coll), rho=m["rho"], ux=m["ux"],
+             uy=m["uy"], uz=m["uz"], forces=hist)
+
+
+def tgv_case(R):
+    c = W.taylor_green(L=12, u0=0.04, tau=0.56, q=19, collision=2)
+    g = oracle.RefGrid3D(c.nx, c.ny, c.nz, c.tau)
+    R.ref3d_set_periodic(g._h, 1)
+    g.init_fields(c.rho, c.ux, c.uy, c.uz)
+    f0 = g.f()
+    g.step(60, 2)
+    m = g.macro()
+    save("tgv3d_mrt", f0=f0, steps=np.int32(60), tau=np.float32(c.tau), rho=m["rho"], ux=m["ux"], uy=m["uy"],
+         uz=m["uz"])
+
+
+def percall_cases(R):
+    """Inputs and outputs of single kernel calls (per-call drop-in parity)."""
+    F = np.float32
+    rng = lambda seed, n: W.uniform24(seed, n)  # noqa: E731
+    res = {}
+    # collisions
+    for Q, pref in ((9, "d2q9"), (19, "d3q19"), (27, "d3q27")):
+        count = 96
+        w = oracle.equilibrium(Q, np.ones(1), np.zeros(1), np.zeros(1), np.zeros(1) if Q != 9 else None)[:, 0]
+        f = (w[:, None] * (1.0 + 0.2 * (rng(W.BASE_SEED + Q, Q * count).reshape(Q, count) - 0.5))).astype(F)
+        ct = np.zeros(count, np.uint8)
+        ct[::7] = 1
+        res[f"{pref}_f"] = f
+        res[f"{pref}_ct"] = ct
+        models = {9: [("bgk", (0.7,)), ("trt", (0.7, 1.2)), ("mrt", (0.7, 1.6))],
+                  19: [("bgk", (0.75,)), ("trt", (0.75, 1.3)), ("mrt", (0.75, 1.2))],
+                  27: [("collide", (0.75, 1.3))]}[Q]
+        for name, taus in models:
+            out = np.zeros_like(f)
+            rho, ux, uy, uz = (np.zeros(count, F) for _ in range(4))
+            fn = getattr(R, f"{pref}_collide_{name}" if Q != 27 else "d3q27_collide")
+            gvec = (1e-5, -2e-5) if Q == 9 else (1e-5, -2e-5, 3e-5)
+            if Q == 9:
+                fn.argtypes = [C.c_void_p] * 6 + [C.c_float] * (len(taus) + 2) + [C.c_int]
+                fn(a(f), a(out), a(ct), a(rho), a(ux), a(uy), *taus, *gvec, count)
+            else:
+                fn.argtypes = [C.c_void_p] * 7 + [C.c_float] * (len(taus) + 3) + [C.c_int]
+                fn(a(f), a(out), a(ct), a(rho), a(ux), a(uy), a(uz), *taus, *gvec, count)
+            key = f"{pref}_{name}"
+            res[f"{key}_out"], res[f"{key}_rho"], res[f"{key}_ux"], res[f"{key}_uy"] = out, rho, ux, uy
+            if Q != 9:
+                res[f"{key}_uz"] = uz
+    # streaming + Zou-He + moments + LES + MEM on a small 2D channel state
+    nx, ny = 20, 12
+    n = nx * ny
+    w9 = oracle.equilibrium(9, np.ones(1), np.zeros(1), np.zeros(1))[:, 0]
+    f = (w9[:, None] * (1.0 + 0.1 * (rng(W.BASE_SEED + 100, 9 * n).reshape(9, n) - 0.5))).astype(F)
+    ct = np.zeros((ny, nx), np.uint8)
+    ct[0, :] = 1
+    ct[ny - 1, :] = 6
+    ct[5:7, 8:10] = 1
+    ct = ct.ravel()
+    res["s2_f"], res["s2_ct"] = f, ct
+    dst = np.zeros_like(f)
+    R.d2q9_stream_with_boundaries.argtypes = [C.c_void_p] * 3 + [C.c_int] * 2 + [C.c_float] * 2
+    R.d2q9_stream_with_boundaries(a(f), a(dst), a(ct), nx, ny, 0.08, 0.0)
+    res["s2_stream"] = dst.copy()
+    per = np.zeros_like(f)
+    R.d2q9_stream_periodic.argtypes = [C.c_void_p] * 2 + [C.c_int] * 2
+    R.d2q9_stream_periodic(a(f), a(per), nx, ny)
+    res["s2_periodic"] = per
+    fz = f.copy()
+    rho, ux, uy = (np.zeros(n, F) for _ in range(3))
+    R.d2q9_apply_zou_he_inflow_west.argtypes = [C.c_void_p] * 4 + [C.c_float] * 2 + [C.c_int] * 2
+    R.d2q9_apply_zou_he_inflow_west(a(fz), a(rho), a(ux), a(uy), 0.05, 0.01, nx, ny)
+    R.d2q9_apply_zou_he_outflow_east.argtypes = [C.c_void_p] * 4 + [C.c_float] + [C.c_int] * 2
+    R.d2q9_apply_zou_he_outflow_east(a(fz), a(rho), a(ux), a(uy), 1.01, nx, ny)
+    res["s2_zh_f"], res["s2_zh_rho"], res["s2_zh_ux"], res["s2_zh_uy"] = fz, rho, ux, uy
+    rho, ux, uy, sp = (np.zeros(n, F) for _ in range(4))
+    R.d2q9_compute_macroscopic_moments_forced.argtypes = [C.c_void_p] * 4 + [C.c_float] * 2 + [C.c_int]
+    R.d2q9_compute_macroscopic_moments_forced(a(f), a(rho), a(ux), a(uy), 1e-4, -2e-4, n)
+    R.d2q9_compute_velocity_magnitude.argtypes = [C.c_void_p] * 3 + [C.c_int]
+    R.d2q9_compute_velocity_magnitude(a(ux), a(uy), a(sp), n)
+    res["s2_mf_rho"], res["s2_mf_ux"], res["s2_mf_uy"], res["s2_speed"] = rho, ux, uy, sp
+    tau_eff = np.zeros(n, F)
+    R.d2q9_compute_smagorinsky_tau.argtypes = [C.c_void_p] * 5 + [C.c_float] * 2 + [C.c_int]
+    R.d2q9_compute_smagorinsky_tau(a(f), a(rho), a(ux), a(uy), a(tau_eff), 0.52, 0.17, n)
+    res["s2_tau_eff"] = tau_eff
+    fx, fy, tz = C.c_float(), C.c_float(), C.c_float()
+    R.d2q9_compute_momentum_exchange_forces.argtypes = [C.c_void_p] * 2 + [C.c_int] * 2 + [C.c_float] * 3 + [C.c_void_p] * 3
+    R.d2q9_compute_momentum_exchange_forces(a(f), a(ct), nx, ny, 8.5, 5.5, 4.0, C.byref(fx), C.byref(fy), C.byref(tz))
+    res["s2_mem"] = np.array([fx.value, fy.value, tz.value], F)
+    # 3D streaming with walls + BFL + MEM
+    nx, ny, nz = 10, 8, 6
+    n = nx * ny * nz
+    w19 = oracle.equilibrium(19, np.ones(1), np.zeros(1), np.zeros(1), np.zeros(1))[:, 0]
+    f = (w19[:, None] * (1.0 + 0.1 * (rng(W.BASE_SEED + 200, 19 * n).reshape(19, n) - 0.5))).astype(F)
+    ct = np.zeros((nz, ny, nx), np.uint8)
+    ct[2:4, 3:5, 4:6] = 1
+    ct[:, ny - 1, :] = 6
+    ct = ct.ravel()
+    res["s3_f"], res["s3_ct"] = f, ct
+    dst = np.zeros_like(f)
+    R.d3q19_stream_with_boundaries.argtypes = [C.c_void_p] * 3 + [C.c_int] * 3 + [C.c_float] * 3
+    R.d3q19_stream_with_boundaries(a(f), a(dst), a(ct), nx, ny, nz, 0.05, 0.0, 0.02)
+    res["s3_stream"] = dst.copy()
+    per = np.zeros_like(f)
+    R.d3q19_stream_periodic.argtypes = [C.c_void_p] * 2 + [C.c_int] * 3
+    R.d3q19_stream_periodic(a(f), a(per), nx, ny, nz)
+    res["s3_periodic"] = per
+    links = [(i, q) for i in range(n) if ct[i] == 0 for q in range(1, 19)]
+    xs = lambda i: (i % nx, (i // nx) % ny, i // (nx * ny))  # noqa: E731
+    lat = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1], [1, 1, 0],
+                    [-1, 1, 0], [1, -1, 0], [-1, -1, 0], [1, 0, 1], [-1, 0, 1], [1, 0, -1], [-1, 0, -1], [0, 1, 1],
+                    [0, -1, 1], [0, 1, -1], [0, -1, -1]])
+    sel = []
+    for i, q in links:
+        x, y, z = xs(i)
+        xn, yn, zn = (x + lat[q, 0]) % nx, y + lat[q, 1], z + lat[q, 2]
+        if 0 <= yn < ny and 0 <= zn < nz and ct[(zn * ny + yn) * nx + xn] == 1:
+            sel.append((i, q))
+    idx = np.array([s[0] for s in sel], np.int32)
+    qd = np.array([s[1] for s in sel], np.int32)
+    nl = len(idx)
+    delta = (0.05 + 0.9 * rng(W.BASE_SEED + 300, nl)).astype(F)
+    uwx, uwy, uwz = (0.01 * (rng(W.BASE_SEED + 301, nl) - 0.5)).astype(F), np.zeros(nl, F), np.zeros(nl, F)
+    fb = dst.copy()
+    R.d3q19_apply_curved_bfl.argtypes = [C.c_void_p] * 8 + [C.c_int] * 4
+    R.d3q19_apply_curved_bfl(a(fb), a(f), a(idx), a(qd), a(delta), a(uwx), a(uwy), a(uwz), nx, ny, nz, nl)
+    res.update(s3_bfl_idx=idx, s3_bfl_q=qd, s3_bfl_delta=delta, s3_bfl_uwx=uwx, s3_bfl_out=fb)
+    fx, fy, fz = C.c_float(), C.c_float(), C.c_float()
+    R.d3q19_compute_momentum_exchange_forces.argtypes = [C.c_void_p] * 2 + [C.c_int] * 3 + [C.c_float] * 4 + [C.c_void_p] * 3
+    R.d3q19_compute_momentum_exchange_forces(a(f), a(ct), nx, ny, nz, 4.5, 3.5, 2.5, 0.0, C.byref(fx), C.byref(fy),
+                                             C.byref(fz))
+    res["s3_mem"] = np.array([fx.value, fy.value, fz.value], F)
+    rho, ux, uy, uz, tau_eff = (np.zeros(n, F) for _ in range(5))
+    R.d3q19_compute_macroscopic_moments.argtypes = [C.c_void_p] * 5 + [C.c_int]
+    R.d3q19_compute_macroscopic_moments(a(f), a(rho), a(ux), a(uy), a(uz), n)
+    R.d3q19_compute_smagorinsky_tau.argtypes = [C.c_void_p] * 6 + [C.c_float] * 2 + [C.c_int]
+    R.d3q19_compute_smagorinsky_tau(a(f), a(rho), a(ux), a(uy), a(uz), a(tau_eff), 0.52, 0.17, n)
+    res.update(s3_rho=rho, s3_ux=ux, s3_uy=uy, s3_uz=uz, s3_tau_eff=tau_eff)
+    # D3Q27 periodic stream
+    f27 = rng(W.BASE_SEED + 400, 27 * n).reshape(27, n).astype(F)
+    per = np.zeros_like(f27)
+    R.d3q27_stream_periodic.argtypes = [C.c_void_p] * 2 + [C.c_int] * 3
+    R.d3q27_stream_periodic(a(f27), a(per), nx, ny, nz)
+    res.update(s27_f=f27, s27_periodic=per)
+    # thermal
+    nx, ny = 12, 8
+    n = nx * ny
+    gi = (w9[:, None] * (0.5 + rng(W.BASE_SEED + 500, 9 * n).reshape(9, n))).astype(F)
+    ctt = np.zeros(n, np.uint8)
+    ctt[5] = 1
+    ux = (0.02 * (rng(W.BASE_SEED + 501, n) - 0.5)).astype(F)
+    uy = (0.02 * (rng(W.BASE_SEED + 502, n) - 0.5)).astype(F)
+    go = np.zeros_like(gi)
+    T = np.zeros(n, F)
+    R.thermal_collide_d2q9.argtypes = [C.c_void_p] * 6 + [C.c_float, C.c_int]
+    R.thermal_collide_d2q9(a(gi), a(go), a(ctt), a(ux), a(uy), a(T), 0.7, n)
+    gw = go.copy()
+    R.thermal_apply_isothermal_wall.argtypes = [C.c_void_p] + [C.c_int] * 3 + [C.c_float]
+    R.thermal_apply_isothermal_wall(a(gw), nx, ny, 0, 1.0)
+    gy = np.full(n, 1e-5, F)
+    R.thermal_compute_buoyancy_force_2d.argtypes = [C.c_void_p] * 2 + [C.c_float] * 3 + [C.c_int]
+    R.thermal_compute_buoyancy_force_2d(a(T), a(gy), 0.5, 0.01, 0.1, n)
+    res.update(th_g=gi, th_ct=ctt, th_ux=ux, th_uy=uy, th_out=go, th_T=T, th_wall=gw, th_gy=gy)
+    save("percall", **res)
+
+
+def kat_cases(R):
+    # Strouhal FFT KAT (tests/unit/test_forces_momentum_exchange.cpp:71-91)
+    t = np.arange(512, dtype=np.float32)
+    sig = (np.float32(0.35) * np.sin(np.float32(6.2831855) * np.float32(0.025) * t) +
+           np.float32(0.02) * np.cos(np.float32(6.2831855) * np.float32(0.1) * t)).astype(np.float32)
+    f = R.ref_strouhal_frequency(a(sig), len(sig), 1.0)
+    save("kat", strouhal_signal=sig, strouhal_freq=np.float32(f))
+
+
+def main():
+    R = oracle.ref()
+    if R is None:
+        raise SystemExit("reference library unavailable: run oracle/build_ref.py where the reference sources exist")
+    cylinder_cases(R)
+    cavity_case(R)
+    poiseuille_case(R)
+    sphere_cases(R)
+    tgv_case(R)
+    percall_cases(R)
+    kat_cases(R)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,291 @@
+"""Fused GPU engine vs the reference (golden fixtures) and the CPU oracle.
+
+Tolerances (FP32 arithmetic on both sides, different summation orders):
+  * relative L2 of the velocity field (components stacked) <= 1e-5
+  * relative L2 of density <= 1e-5
+  * momentum-exchange force history (C_D, C_L stacked) relative L2 <= 1e-4
+Every case also reports its error against the FP64 oracle next to the
+reference's own error against it.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2, vel_rel_l2
+
+pytestmark = pytest.mark.gpu
+
+wb = pytest.importorskip("wake_b200")
+import oracle  # noqa: E402
+from wake_b200 import workloads as W  # noqa: E402
+
+U_TOL = 1e-5
+RHO_TOL = 1e-5
+FORCE_TOL = 1e-4
+
+
+def _oracle_2d(types, nx, ny, f0, tau, collision, steps, prec, inflow=False, lid=None, g=(0.0, 0.0, 0.0), mem=None):
+    o = oracle.OracleGrid(9, nx, ny, 1, prec)
+    kw = dict(collision=collision, tau=tau, g=g)
+    if inflow:
+        kw.update(inflow=1, outflow=1, u_in=(0.05, 0.0, 0.0), rho_out=1.0)
+    if lid is not None:
+        kw.update(u_wall=(lid, 0.0, 0.0))
+    if mem is not None:
+        kw.update(mem=1, center=(mem[0], mem[1], 0.0), r_max=mem[2])
+    o.configure(**kw)
+    o.set_cell_types(types)
+    o.set_state(f0)
+    hist = o.step(steps, forces=mem is not None)
+    return o.macro(), hist
+
+
+@pytest.mark.parametrize("tag,collision", [("bgk", wb.BGK), ("trt", wb.TRT), ("mrt", wb.MRT)])
+def test_cylinder_channel_matches_reference(golden, tag, collision):
+    d = golden(f"cyl2d_{tag}")
+    nx, ny, steps, tau = 64, 32, int(d["steps"]), float(d["tau"])
+    g = wb.LatticeGrid2D(nx, ny, tau, les_applies=False)
+    wb.check(wb.lib.wake_grid_set_inflow_west(g.handle, 0.05, 0.0, 0.0))
+    g.set_outflow_east(1.0)
+    g.set_cell_types(d["types"])
+    g.set_populations(d["f0"])
+    g.enable_forces(16.0, 16.0, 0.0, 12.0)
+    g.step(collision, n=steps)
+    g.synchronize()
+    m = g.macro()
+    hist = g.force_history()
+    assert hist.shape == (steps, 3)
+    ref = {k: d[k] for k in ("rho", "ux", "uy")}
+    e_u, e_rho = vel_rel_l2(m, ref), rel_l2(m["rho"], ref["rho"])
+    q = 0.5 * 1.0 * 0.05 ** 2 * 8.0
+    e_f = rel_l2(hist[:, :2] / q, d["forces"][:, :2] / q)
+    e_cd_last = abs(hist[-1, 0] - d["forces"][-1, 0]) / abs(d["forces"][-1, 0])
+    e_fsrc = rel_l2(g.f_src_data(), d["f_end"])
+    m64, h64 = _oracle_2d(d["types"], nx, ny, d["f0"], tau, collision, steps, 64, inflow=True, mem=(16.0, 16.0, 12.0))
+    print(f"[cyl2d {tag}] gpu-vs-ref u {e_u:.2e} rho {e_rho:.2e} force {e_f:.2e} CD(last) {e_cd_last:.2e} "
+          f"f_src {e_fsrc:.2e} | vs FP64: gpu {vel_rel_l2(m, m64):.2e} ref {vel_rel_l2(ref, m64):.2e}")
+    assert e_u <= U_TOL and e_rho <= RHO_TOL
+    assert e_f <= FORCE_TOL and e_cd_last <= FORCE_TOL
+    assert e_fsrc <= 1e-6
+    # as accurate as the reference against the FP64 oracle
+    assert vel_rel_l2(m, m64) <= 2.0 * vel_rel_l2(ref, m64) + 1e-6
+
+
+def test_lid_driven_cavity_matches_reference(golden):
+    d = golden("cavity2d_mrt")
+    n = 32
+    g = wb.LatticeGrid2D(n, n, float(d["tau"]), les_applies=False)
+    g.set_moving_wall_north(float(d["lid"]))
+    g.set_cell_types(d["types"])
+    g.set_populations(d["f0"])
+    g.step(wb.MRT, n=int(d["steps"]))
+    m = g.macro()
+    ref = {k: d[k] for k in ("rho", "ux", "uy")}
+    e_u = vel_rel_l2(m, ref)
+    print(f"[cavity mrt] u {e_u:.2e} rho {rel_l2(m['rho'], ref['rho']):.2e}")
+    assert e_u <= U_TOL and rel_l2(m["rho"], ref["rho"]) <= RHO_TOL
+
+
+def test_body_force_channel_matches_reference(golden):
+    d = golden("poiseuille2d_trt")
+    g = wb.LatticeGrid2D(8, 33, float(d["tau"]), les_applies=False)
+    g.set_cell_types(d["types"])
+    g.set_populations(d["f0"])
+    g.step(wb.TRT, gx=float(d["gx"]), n=int(d["steps"]))
+    m = g.macro()
+    e_u = vel_rel_l2(m, {k: d[k] for k in ("ux", "uy")})
+    print(f"[poiseuille trt] u {e_u:.2e}")
+    assert e_u <= U_TOL
+
+
+@pytest.mark.parametrize("tag,collision", [("bgk", wb.BGK), ("trt", wb.TRT), ("mrt", wb.MRT)])
+def test_sphere_bfl_matches_reference(golden, tag, collision):
+    d = golden(f"sphere3d_{tag}")
+    nx, ny, nz = 24, 16, 16
+    n = nx * ny * nz
+    g = wb.LatticeGrid3D(nx, ny, nz, float(d["tau"]), les_applies=False)
+    g.set_cell_types(d["types"])
+    nl = g.build_curved_sphere_links(8.0, 8.0, 8.0, 4.0)
+    idx, q, delta = g.curved_links()
+    # the engine's link builder reproduces the reference's links exactly
+    assert nl == len(d["links_idx"])
+    assert np.array_equal(idx, d["links_idx"]) and np.array_equal(q, d["links_q"])
+    assert np.max(np.abs(delta - d["links_delta"])) <= 1e-6
+    f0 = np.repeat(d["f0_node"][:, None], n, axis=1)
+    g.set_populations(f0)
+    g.enable_forces(8.0, 8.0, 8.0, 8.0)
+    g.step(collision, n=int(d["steps"]))
+    m = g.macro()
+    hist = g.force_history()
+    ref = {k: d[k] for k in ("rho", "ux", "uy", "uz")}
+    e_u = vel_rel_l2(m, ref, ("ux", "uy", "uz"))
+    e_rho = rel_l2(m["rho"], ref["rho"])
+    e_f = rel_l2(hist, d["forces"])
+    print(f"[sphere3d {tag}] links {nl} u {e_u:.2e} rho {e_rho:.2e} force {e_f:.2e}")
+    assert e_u <= U_TOL and e_rho <= RHO_TOL and e_f <= FORCE_TOL
+
+
+def test_taylor_green_d3q19_mrt_matches_reference(golden):
+    d = golden("tgv3d_mrt")
+    L = 12
+    g = wb.LatticeGrid3D(L, L, L, float(d["tau"]), les_applies=False)
+    g.set_periodic_axes(True, True)
+    g.set_populations(d["f0"])
+    g.step(wb.MRT, n=int(d["steps"]))
+    m = g.macro()
+    e_u = vel_rel_l2(m, {k: d[k] for k in ("ux", "uy", "uz")}, ("ux", "uy", "uz"))
+    print(f"[tgv d3q19 mrt] u {e_u:.2e}")
+    assert e_u <= U_TOL and rel_l2(m["rho"], d["rho"]) <= RHO_TOL
+
+
+def _run_case_gpu(case, steps, storage="f32"):
+    g = W.build_grid(case, storage=storage)
+    g.step(case.collision, use_les=case.les, smag_const=case.cs_smag, n=steps)
+    g.synchronize()
+    return g
+
+
+def _run_case_oracle(case, steps, prec, links=None):
+    o = oracle.OracleGrid(case.q, case.nx, case.ny, case.nz, prec)
+    kw = dict(collision=case.collision, tau=case.tau, les=int(case.les), cs_smag=case.cs_smag,
+              periodic_y=int(case.periodic_y), periodic_z=int(case.periodic_z))
+    if case.inflow is not None:
+        kw.update(inflow=1, u_in=case.inflow)
+    if case.outflow is not None:
+        kw.update(outflow=1, rho_out=case.outflow)
+    if case.mem is not None:
+        kw.update(mem=1, center=case.mem[:3], r_max=case.mem[3])
+    o.configure(**kw)
+    o.set_cell_types(case.types)
+    f0 = oracle.equilibrium(case.q, case.rho, case.ux, case.uy, case.uz if case.q != 9 else None, prec=32)
+    o.set_state(f0.astype(np.float32))
+    if links is not None:
+        o.set_links(*links)
+    hist = o.step(steps, forces=case.mem is not None)
+    return o, hist
+
+
+def test_sphere_extended_matches_oracle():
+    """Zou-He faces, periodic y/z, applied Smagorinsky LES, TRT, BFL (no reference counterpart)."""
+    case = W.sphere_channel(nx=40, ny=24, nz=24, radius=5.0, center=(14.0, 12.0, 12.0), tau=0.52, collision=wb.TRT,
+                            les=True, cs_smag=0.17)
+    steps = 80
+    g = _run_case_gpu(case, steps)
+    links = g.curved_links()
+    m = g.macro()
+    hist = g.force_history()
+    o32, h32 = _run_case_oracle(case, steps, 32, links)
+    o64, h64 = _run_case_oracle(case, steps, 64, links)
+    m32, m64 = o32.macro(), o64.macro()
+    e32 = vel_rel_l2(m, m32, ("ux", "uy", "uz"))
+    e64 = vel_rel_l2(m, m64, ("ux", "uy", "uz"))
+    ef = rel_l2(hist, h32)
+    print(f"[sphere extended] vs oracle-fp32 u {e32:.2e} force {ef:.2e} | vs FP64 u {e64:.2e} "
+          f"(oracle-fp32 vs FP64 {vel_rel_l2(m32, m64, ('ux', 'uy', 'uz')):.2e})")
+    assert e32 <= U_TOL and rel_l2(m["rho"], m32["rho"]) <= RHO_TOL and ef <= FORCE_TOL
+    # inlet nodes carry the prescribed velocity
+    ux = m["ux"].reshape(case.nz, case.ny, case.nx)
+    assert np.allclose(ux[:, :, 0], 0.05, atol=1e-6)
+
+
+@pytest.mark.parametrize("collision", [wb.TRT, wb.MRT])
+def test_d3q27_taylor_green_matches_oracle(collision):
+    case = W.taylor_green(L=16, u0=0.04, tau=0.51, q=27, collision=collision)
+    steps = 60
+    g = _run_case_gpu(case, steps)
+    m = g.macro()
+    o32, _ = _run_case_oracle(case, steps, 32)
+    o64, _ = _run_case_oracle(case, steps, 64)
+    m32, m64 = o32.macro(), o64.macro()
+    e32 = vel_rel_l2(m, m32, ("ux", "uy", "uz"))
+    print(f"[d3q27 coll={collision}] vs oracle-fp32 {e32:.2e} vs FP64 {vel_rel_l2(m, m64, ('ux', 'uy', 'uz')):.2e}")
+    assert e32 <= U_TOL
+
+
+@pytest.mark.parametrize("storage,tol", [("f16", 1e-3), ("bf16", 1e-2)])
+def test_shifted_storage_error_vs_fp64(storage, tol):
+    """FP16 / BF16 storage of f/w - 1 with FP32 arithmetic: velocity error vs the FP64 oracle."""
+    case = W.taylor_green(L=32, u0=0.04, tau=0.51, q=27, collision=wb.MRT)
+    steps = 100
+    g = _run_case_gpu(case, steps, storage=storage)
+    m = g.macro()
+    o64, _ = _run_case_oracle(case, steps, 64)
+    e = vel_rel_l2(m, o64.macro(), ("ux", "uy", "uz"))
+    print(f"[{storage} d3q27 tgv] velocity rel-L2 vs FP64 {e:.2e}")
+    assert e <= tol
+
+
+def test_shifted_storage_drag_vs_fp64():
+    """FP16 storage: C_D within 0.5% of the FP64 oracle on a cylinder channel."""
+    case = W.cylinder_channel(nx=96, ny=48, diameter=10, cx=24, cy=24, tau=0.56, collision=wb.TRT)
+    steps = 300
+    g = _run_case_gpu(case, steps, storage="f16")
+    hist = g.force_history()
+    _, h64 = _run_case_oracle(case, steps, 64)
+    cd, cd64 = hist[-50:, 0].mean(), h64[-50:, 0].mean()
+    print(f"[f16 cylinder] C_D {cd:.6f} vs FP64 {cd64:.6f} ({abs(cd - cd64) / abs(cd64):.2e})")
+    assert abs(cd - cd64) <= 5e-3 * abs(cd64)
+
+
+def test_geometry_change_after_steps_matches_oracle():
+    """Cell types changed mid-run: the engine re-derives f_src like the reference keeps it."""
+    case = W.cylinder_channel(nx=48, ny=24, diameter=6, cx=12, cy=12, tau=0.6, collision=wb.BGK)
+    g = _run_case_gpu(case, 20)
+    g.set_cell_type(30, 12, wb.SOLID)
+    g.step(wb.BGK, n=20)
+    m = g.macro()
+    o, _ = _run_case_oracle(case, 20, 32)
+    t = case.types.copy()
+    t[12 * 48 + 30] = 1
+    o.set_cell_types(t)
+    o.step(20)
+    assert vel_rel_l2(m, o.macro()) <= U_TOL
+
+
+def test_graph_replay_equals_plain_steps():
+    case = W.cylinder_channel(nx=64, ny=32, diameter=8, cx=16, cy=16, tau=0.56, collision=wb.TRT)
+    a = _run_case_gpu(case, 40)
+    b = W.build_grid(case)
+    b.use_graph(8)
+    b.step(case.collision, n=40)
+    ma, mb = a.macro(), b.macro()
+    assert np.array_equal(ma["ux"], mb["ux"]) and np.array_equal(ma["rho"], mb["rho"])
+    assert np.array_equal(a.force_history(), b.force_history())
+
+
+def test_forces_are_deterministic():
+    case = W.cylinder_channel(nx=64, ny=32, diameter=8, cx=16, cy=16, tau=0.56, collision=wb.TRT)
+    h1 = _run_case_gpu(case, 30).force_history()
+    h2 = _run_case_gpu(case, 30).force_history()
+    assert np.array_equal(h1, h2)
+
+
+def test_block_shape_does_not_change_results():
+    case = W.sphere_channel(nx=40, ny=16, nz=16, radius=4.0, center=(12.0, 8.0, 8.0), tau=0.55, collision=wb.TRT)
+    a = _run_case_gpu(case, 20)
+    b = W.build_grid(case)
+    wb.check(wb.lib.wake_grid_set_block(b.handle, 32))
+    b.step(case.collision, use_les=case.les, smag_const=case.cs_smag, n=20)
+    assert np.array_equal(a.macro()["ux"], b.macro()["ux"])
+    assert rel_l2(a.force_history(), b.force_history()) <= 1e-12
+
+
+def test_diagnostics_fp64():
+    case = W.taylor_green(L=16, u0=0.04, tau=0.8, q=19, collision=wb.MRT)
+    g = _run_case_gpu(case, 10)
+    m = g.macro()
+    mass, ke, vmax = g._diag()
+    assert abs(mass - m["rho"].astype(np.float64).sum()) <= 1e-9 * mass
+    ke_ref = (0.5 * m["rho"].astype(np.float64) * m["speed"].astype(np.float64) ** 2).sum()
+    assert abs(ke - ke_ref) <= 1e-9 * ke_ref
+    assert abs(vmax - m["speed"].max()) <= 1e-7
+
+
+def test_numeric_failure_is_reported():
+    """A non-finite population is reported as WAKE_ERR_NUMERIC by the status word, not a fault."""
+    g = wb.LatticeGrid2D(32, 16, 0.6)
+    f0 = oracle.equilibrium(9, np.ones(512), np.zeros(512), np.zeros(512)).astype(np.float32)
+    f0[1, 100] = np.nan
+    g.set_populations(f0)
+    g.step(wb.BGK, n=2)
+    with pytest.raises(wb.WakeError):
+        g.synchronize()

@@ -1,0 +1,1020 @@
+// Host engine of the fused lattice update: one resident lattice per
+// wake_grid handle (C ABI in include/wake_gpu.h).
+//
+// Mirrors the reference's LatticeGrid2D / LatticeGrid3D (src/grid/lattice_grid_2d.cpp,
+// src/grid/lattice_grid_3d.cpp): same geometry setters, same step semantics,
+// same readable state (f_src, rho, u, speed) after every step. The difference
+// is where the work happens: the state lives in HBM as two SoA population
+// buffers and one step is one kernel launch (stream_collide.cuh).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "wake_gpu.h"
+
+namespace wk {
+
+namespace {
+thread_local std::string t_err;
+thread_local int t_code = 0;
+}  // namespace
+
+int set_error(int code, const std::string& msg) {
+    t_err = msg;
+    t_code = code;
+    return code;
+}
+void clear_error() {
+    t_err.clear();
+    t_code = 0;
+}
+
+// ---------------------------------------------------------------- host lattice tables
+struct HostLat {
+    int Q = 0, D = 0;
+    int cx[27], cy[27], cz[27], opp[27];
+    float w[27];
+    explicit HostLat(int q) : Q(q) {
+        auto fill = [&](auto lat) {
+            using L = decltype(lat);
+            D = L::D;
+            for (int k = 0; k < Q; ++k) {
+                cx[k] = L::cx(k);
+                cy[k] = L::cy(k);
+                cz[k] = L::cz(k);
+                opp[k] = L::opp(k);
+                w[k] = L::w(k);
+            }
+        };
+        if (q == 9) fill(Lat<9>{});
+        else if (q == 19) fill(Lat<19>{});
+        else fill(Lat<27>{});
+    }
+};
+
+cudaError_t launch_step_any(int Q, int coll, int store, bool les, const StepArgs& a, const Launch& L) {
+    if (Q == 9) return launch_step_q9(coll, store, les, a, L);
+    if (Q == 19) return launch_step_q19(coll, store, les, a, L);
+    return launch_step_q27(coll, store, les, a, L);
+}
+cudaError_t launch_initial_any(int Q, int coll, int store, bool les, const float* f0, void* a, void* b,
+                               const uint8_t* flags, const Geo& geo, const Physics& phys, const Launch& L) {
+    if (Q == 9) return launch_initial_q9(coll, store, les, f0, a, b, flags, geo, phys, L);
+    if (Q == 19) return launch_initial_q19(coll, store, les, f0, a, b, flags, geo, phys, L);
+    return launch_initial_q27(coll, store, les, f0, a, b, flags, geo, phys, L);
+}
+cudaError_t launch_materialise_any(int Q, int store, const void* fin, const uint8_t* flags, const Geo& geo,
+                                   const Links& links, const Physics& phys, const Out& out, const Launch& L,
+                                   int direct) {
+    if (Q == 9) return launch_materialise_q9(store, fin, flags, geo, links, phys, out, L, direct);
+    if (Q == 19) return launch_materialise_q19(store, fin, flags, geo, links, phys, out, L, direct);
+    return launch_materialise_q27(store, fin, flags, geo, links, phys, out, L, direct);
+}
+cudaError_t launch_flags_any(int Q, const uint8_t* types, uint8_t* flags, const Geo& geo, const FlagCfg& cfg,
+                             const Launch& L) {
+    if (Q == 9) return launch_flags_q9(types, flags, geo, cfg, L);
+    if (Q == 19) return launch_flags_q19(types, flags, geo, cfg, L);
+    return launch_flags_q27(types, flags, geo, cfg, L);
+}
+cudaError_t launch_block_marks_any(int Q, const uint8_t* flags, int* marks, const Geo& geo, const Launch& L) {
+    if (Q == 9) return launch_block_marks_q9(flags, marks, geo, L);
+    if (Q == 19) return launch_block_marks_q19(flags, marks, geo, L);
+    return launch_block_marks_q27(flags, marks, geo, L);
+}
+
+// ---------------------------------------------------------------- small kernels
+__global__ void k_link_marks(const int* __restrict__ node, int n, uint8_t* __restrict__ flags,
+                             int* __restrict__ node_start) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = node[k];
+    if (k == 0 || node[k - 1] != i) {
+        node_start[i] = k;
+        flags[i] = static_cast<uint8_t>((flags[i] | FL_BFL) & ~FL_FAST);
+    }
+}
+
+// Deterministic per-block partial sums for the diagnostics:
+// [0] mass over Fluid, [1] kinetic energy over Fluid, [2] max speed over Fluid,
+// [3] mass over every non-solid cell.
+__global__ void k_diag_partials(const float* __restrict__ rho, const float* __restrict__ speed,
+                                const uint8_t* __restrict__ flags, long long n, double* __restrict__ part) {
+    __shared__ double s[4][256];
+    double m = 0.0, ke = 0.0, mx = 0.0, mall = 0.0;
+    for (long long i = blockIdx.x * 256ll + threadIdx.x; i < n; i += 256ll * gridDim.x) {
+        const uint8_t t = flags[i] & FL_TYPE;
+        if (t == CT_FLUID) {
+            const double r = rho[i], sp = speed[i];
+            m += r;
+            ke += 0.5 * r * sp * sp;
+            mx = fmax(mx, sp);
+        }
+        if (t != CT_SOLID) mall += rho[i];
+    }
+    s[0][threadIdx.x] = m;
+    s[1][threadIdx.x] = ke;
+    s[2][threadIdx.x] = mx;
+    s[3][threadIdx.x] = mall;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            s[0][threadIdx.x] += s[0][threadIdx.x + o];
+            s[1][threadIdx.x] += s[1][threadIdx.x + o];
+            s[2][threadIdx.x] = fmax(s[2][threadIdx.x], s[2][threadIdx.x + o]);
+            s[3][threadIdx.x] += s[3][threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 4; ++c) part[4 * blockIdx.x + c] = s[c][0];
+}
+
+cudaError_t launch_link_marks(const int* link_node, int n_links, uint8_t* flags, int* node_start,
+                              cudaStream_t stream) {
+    if (n_links <= 0) return cudaSuccess;
+    k_link_marks<<<(n_links + 255) / 256, 256, 0, stream>>>(link_node, n_links, flags, node_start);
+    return cudaGetLastError();
+}
+
+}  // namespace wk
+
+using namespace wk;
+
+// ==================================================================== grid
+struct wake_grid {
+    int Q = 0, D = 0, nx = 0, ny = 0, nz = 0, storage = 0;
+    long long N = 0, pitch = 0;
+    std::size_t elem = 4;
+    HostLat lat{9};
+
+    DevMem A, B;       // state buffers
+    int cur = 0;       // 0: A holds the current state, 1: B
+    bool direct = true;  // the non-current buffer holds f^k itself (right after initialisation)
+    DevMem d_types, d_flags, d_status, d_nodestart;
+    std::vector<uint8_t> types;
+    bool geom_dirty = true;
+
+    int collision = WAKE_MRT, les = 0;
+    Physics phys{};
+    int inflow = 0, outflow = 0, lid = 0, periodic_y = 0, periodic_z = 0;
+    float uin[3] = {0.f, 0.f, 0.f}, rho_out = 1.0f, uw[3] = {0.f, 0.f, 0.f};
+
+    std::vector<int> link_node, link_q;
+    std::vector<float> link_delta, link_uw;  // uw: 3 per link
+    DevMem d_link_node, d_link_q, d_link_delta, d_link_mom;
+    int dev_links = 0;         // links currently on the device (the flags refer to these)
+    bool links_dirty = false;  // host links differ from the device copy
+
+    int mem_on = 0, hist_cap = 0, n_slots = 0;
+    float center[3] = {0.f, 0.f, 0.f}, rmax = 0.f;
+    DevMem d_block_slot, d_partial, d_counters, d_hist;
+
+    int tpb = 0, xchunks = 1, rows = 1;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    long long k = 0;
+
+    DevMem m_f, m_rho, m_ux, m_uy, m_uz, m_speed, m_diag;
+
+    // CUDA graph of `graph_steps` fused steps starting from buffer parity graph_cur
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0, graph_cur = -1;
+    float graph_g[3] = {0.f, 0.f, 0.f};
+    bool graph_ok = false;
+
+    explicit wake_grid(int q) : lat(q) {}
+    ~wake_grid() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+
+    void* buf(int which) { return which == 0 ? A.p : B.p; }
+
+    Geo geo() const {
+        Geo g{};
+        g.nx = nx;
+        g.ny = ny;
+        g.nz = nz;
+        g.periodic_y = (D == 3) ? periodic_y : 0;
+        g.periodic_z = (D == 3) ? periodic_z : 0;
+        g.pitch = pitch;
+        for (int a = 0; a < 3; ++a) g.uin[a] = uin[a];
+        g.rho_out = rho_out;
+        for (int q = 0; q < Q; ++q) {
+            // 2 w_q rho_0 / cs^2 (c_q . u_w) in the reference's float order (d2q9_streaming.ispc:49-53)
+            const float ci_uw = float(lat.cx[q]) * uw[0] + float(lat.cy[q]) * uw[1] + float(lat.cz[q]) * uw[2];
+            g.mom[q] = lid ? 2.0f * lat.w[q] * 1.0f * 3.0f * ci_uw : 0.0f;
+        }
+        return g;
+    }
+    Links links() const {
+        Links l{};
+        l.node_start = d_nodestart.as<int>();
+        l.node = d_link_node.as<int>();
+        l.q = d_link_q.as<int>();
+        l.delta = d_link_delta.as<float>();
+        l.mom = d_link_mom.as<float>();
+        l.count = dev_links;
+        return l;
+    }
+    Launch launch() const { return Launch{tpb, xchunks, rows, stream}; }
+    int blocks() const { return rows * xchunks; }
+
+    void invalidate_graph() { graph_ok = false; }
+
+    void choose_block(int want) {
+        const int full = ((nx + 31) / 32) * 32;
+        if (want > 0) tpb = want;
+        else if (full <= 512) tpb = full;
+        else {
+            int best = 256;
+            long long best_waste = -1;
+            for (int t : {256, 384, 512}) {
+                const long long chunks = (nx + t - 1) / t;
+                const long long waste = chunks * t - nx;
+                if (best_waste < 0 || waste < best_waste) {
+                    best = t;
+                    best_waste = waste;
+                }
+            }
+            tpb = best;
+        }
+        xchunks = (nx + tpb - 1) / tpb;
+        rows = ny * nz;
+    }
+};
+
+namespace {
+
+bool valid_grid(wake_grid* g) {
+    if (!g) {
+        set_error(WAKE_ERR_INVALID, "null wake_grid handle");
+        return false;
+    }
+    return true;
+}
+
+long long idx3(const wake_grid* g, int x, int y, int z) {
+    return (static_cast<long long>(z) * g->ny + y) * g->nx + x;
+}
+
+int upload_links(wake_grid* g);
+
+// Upload types and links, rebuild flags and momentum-exchange slots.
+int rebuild_flags(wake_grid* g) {
+    if (g->links_dirty) {
+        const int r = upload_links(g);
+        if (r) return r;
+        g->links_dirty = false;
+    }
+    WK_CUDA(cudaMemcpyAsync(g->d_types.p, g->types.data(), g->N, cudaMemcpyHostToDevice, g->stream));
+    FlagCfg cfg{};
+    cfg.zh_rule = (g->Q == 9) ? 1 : 2;
+    cfg.inflow = g->inflow;
+    cfg.outflow = g->outflow;
+    cfg.mem_enabled = g->mem_on;
+    for (int a = 0; a < 3; ++a) cfg.center[a] = g->center[a];
+    cfg.r_max = g->rmax;
+    cfg.r_max_sq = g->rmax * g->rmax;
+    const Geo geo = g->geo();
+    WK_CUDA(launch_flags_any(g->Q, g->d_types.as<uint8_t>(), g->d_flags.as<uint8_t>(), geo, cfg, g->launch()));
+    const int nl = g->dev_links;
+    if (nl > 0) {
+        WK_CUDA(g->d_nodestart.ensure(sizeof(int) * g->N));
+        WK_CUDA(cudaMemsetAsync(g->d_nodestart.p, 0xff, sizeof(int) * g->N, g->stream));
+        WK_CUDA(launch_link_marks(g->d_link_node.as<int>(), nl, g->d_flags.as<uint8_t>(), g->d_nodestart.as<int>(),
+                                  g->stream));
+    }
+    if (g->mem_on) {
+        const int nb = g->blocks();
+        DevMem marks;
+        WK_CUDA(marks.ensure(sizeof(int) * nb));
+        WK_CUDA(launch_block_marks_any(g->Q, g->d_flags.as<uint8_t>(), marks.as<int>(), geo, g->launch()));
+        std::vector<int> h(nb);
+        WK_CUDA(cudaMemcpyAsync(h.data(), marks.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, g->stream));
+        WK_CUDA(cudaStreamSynchronize(g->stream));
+        int slot = 0;
+        for (int b = 0; b < nb; ++b) h[b] = h[b] ? slot++ : -1;
+        if (slot == 0) h[0] = slot++;  // no link in range: block 0 still records a zero force every step
+        g->n_slots = slot;
+        WK_CUDA(g->d_block_slot.ensure(sizeof(int) * nb));
+        WK_CUDA(cudaMemcpyAsync(g->d_block_slot.p, h.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, g->stream));
+        WK_CUDA(g->d_partial.ensure(sizeof(double) * 3 * std::max(1, slot)));
+        WK_CUDA(cudaStreamSynchronize(g->stream));  // h goes out of scope
+    }
+    g->geom_dirty = false;
+    g->invalidate_graph();
+    return WAKE_OK;
+}
+
+// Upload the links (sorted by fluid node) and their moving-wall terms.
+int upload_links(wake_grid* g) {
+    const int n = static_cast<int>(g->link_node.size());
+    g->dev_links = 0;
+    if (n == 0) return WAKE_OK;
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return g->link_node[a] < g->link_node[b]; });
+    std::vector<int> node(n), q(n);
+    std::vector<float> delta(n), mom(n);
+    for (int j = 0; j < n; ++j) {
+        const int k = order[j];
+        node[j] = g->link_node[k];
+        q[j] = g->link_q[k];
+        delta[j] = g->link_delta[k];
+        const int qq = q[j];
+        const float ci_uw = float(g->lat.cx[qq]) * g->link_uw[3 * k] + float(g->lat.cy[qq]) * g->link_uw[3 * k + 1] +
+                            float(g->lat.cz[qq]) * g->link_uw[3 * k + 2];
+        // d3q19_curved.ispc:57 (delta < 1/2) and :62 (delta >= 1/2)
+        mom[j] = (delta[j] < 0.5f) ? 2.0f * g->lat.w[qq] * 1.0f * 3.0f * ci_uw
+                                   : (1.0f / delta[j]) * g->lat.w[qq] * 1.0f * 3.0f * ci_uw;
+    }
+    WK_CUDA(g->d_link_node.ensure(sizeof(int) * n));
+    WK_CUDA(g->d_link_q.ensure(sizeof(int) * n));
+    WK_CUDA(g->d_link_delta.ensure(sizeof(float) * n));
+    WK_CUDA(g->d_link_mom.ensure(sizeof(float) * n));
+    WK_CUDA(cudaMemcpyAsync(g->d_link_node.p, node.data(), sizeof(int) * n, cudaMemcpyHostToDevice, g->stream));
+    WK_CUDA(cudaMemcpyAsync(g->d_link_q.p, q.data(), sizeof(int) * n, cudaMemcpyHostToDevice, g->stream));
+    WK_CUDA(cudaMemcpyAsync(g->d_link_delta.p, delta.data(), sizeof(float) * n, cudaMemcpyHostToDevice, g->stream));
+    WK_CUDA(cudaMemcpyAsync(g->d_link_mom.p, mom.data(), sizeof(float) * n, cudaMemcpyHostToDevice, g->stream));
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    g->dev_links = n;
+    return WAKE_OK;
+}
+
+Out scratch_out(wake_grid* g, bool want_f, bool want_macro) {
+    Out o{};
+    if (want_f) o.f = g->m_f.as<float>();
+    if (want_macro) {
+        o.rho = g->m_rho.as<float>();
+        o.ux = g->m_ux.as<float>();
+        o.uy = g->m_uy.as<float>();
+        o.uz = g->m_uz.as<float>();
+        o.speed = g->m_speed.as<float>();
+    }
+    return o;
+}
+
+int ensure_macro(wake_grid* g) {
+    const std::size_t b = sizeof(float) * g->N;
+    WK_CUDA(g->m_rho.ensure(b));
+    WK_CUDA(g->m_ux.ensure(b));
+    WK_CUDA(g->m_uy.ensure(b));
+    WK_CUDA(g->m_uz.ensure(b));
+    WK_CUDA(g->m_speed.ensure(b));
+    return WAKE_OK;
+}
+
+// Write the reference-visible f^k (and/or macroscopic fields) into the scratch buffers.
+int materialise(wake_grid* g, bool want_f, bool want_macro) {
+    if (want_f) WK_CUDA(g->m_f.ensure(sizeof(float) * g->Q * g->pitch));
+    if (want_macro) {
+        const int r = ensure_macro(g);
+        if (r) return r;
+    }
+    const Out o = scratch_out(g, want_f, want_macro);
+    const void* src = g->buf(1 - g->cur);
+    WK_CUDA(launch_materialise_any(g->Q, g->storage, src, g->d_flags.as<uint8_t>(), g->geo(), g->links(), g->phys, o,
+                                   g->launch(), g->direct ? 1 : 0));
+    return WAKE_OK;
+}
+
+// Initial collide from the FP32 populations in m_f (flags must be current).
+int initial_from_scratch(wake_grid* g) {
+    WK_CUDA(launch_initial_any(g->Q, g->collision, g->storage, g->les != 0, g->m_f.as<float>(), g->A.p, g->B.p,
+                               g->d_flags.as<uint8_t>(), g->geo(), g->phys, g->launch()));
+    g->cur = 0;
+    g->direct = true;
+    g->invalidate_graph();
+    return WAKE_OK;
+}
+
+// Bring flags in line with the host geometry. If the cell types changed, the
+// reference-visible state f^k is re-derived with the old flags and the
+// collided buffer rebuilt with the new ones (the reference keeps f_src as is).
+int prepare(wake_grid* g) {
+    if (!g->geom_dirty) return WAKE_OK;
+    int r = materialise(g, true, false);
+    if (r) return r;
+    r = rebuild_flags(g);
+    if (r) return r;
+    return initial_from_scratch(g);
+}
+
+int upload_f0(wake_grid* g, const float* f, cudaMemcpyKind kind) {
+    WK_CUDA(g->m_f.ensure(sizeof(float) * g->Q * g->pitch));
+    WK_CUDA(cudaMemcpy2DAsync(g->m_f.p, sizeof(float) * g->pitch, f, sizeof(float) * g->N, sizeof(float) * g->N,
+                              g->Q, kind, g->stream));
+    if (g->geom_dirty) {
+        const int r = rebuild_flags(g);
+        if (r) return r;
+    }
+    const int r = initial_from_scratch(g);
+    if (r) return r;
+    g->k = 0;
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    return WAKE_OK;
+}
+
+// Host equilibrium in the reference's float order (lattice_grid_2d.cpp:90-119):
+// writes f[q * stride] for q = 0..Q-1.
+void equilibrium(const HostLat& lat, float rho, float ux, float uy, float uz, float* f, long long stride) {
+    const float u_sq = ux * ux + uy * uy + uz * uz;
+    for (int q = 0; q < lat.Q; ++q) {
+        const float ci_u = float(lat.cx[q]) * ux + float(lat.cy[q]) * uy + float(lat.cz[q]) * uz;
+        f[q * stride] = lat.w[q] * rho * (1.0f + 3.0f * ci_u + 4.5f * ci_u * ci_u - 1.5f * u_sq);
+    }
+}
+
+int do_steps(wake_grid* g, int n) {
+    for (int s = 0; s < n; ++s) {
+        StepArgs a{};
+        a.fin = g->buf(g->cur);
+        a.fout = g->buf(1 - g->cur);
+        a.flags = g->d_flags.as<uint8_t>();
+        a.status = g->d_status.as<unsigned>();
+        a.geo = g->geo();
+        a.links = g->links();
+        a.mem.enabled = g->mem_on;
+        if (g->mem_on) {
+            for (int c = 0; c < 3; ++c) a.mem.center[c] = g->center[c];
+            a.mem.r_max = g->rmax;
+            a.mem.r_max_sq = g->rmax * g->rmax;
+            a.mem.block_slot = g->d_block_slot.as<int>();
+            a.mem.partial = g->d_partial.as<double>();
+            a.mem.arrivals = g->d_counters.as<unsigned>();
+            a.mem.hist_step = g->d_counters.as<unsigned>() + 1;
+            a.mem.hist = g->d_hist.as<double>();
+            a.mem.hist_cap = g->hist_cap;
+            a.mem.n_slots = g->n_slots;
+            if (g->n_slots == 0) a.mem.enabled = 0;
+        }
+        a.phys = g->phys;
+        a.xchunks = g->xchunks;
+        WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, a, g->launch()));
+        g->cur ^= 1;
+        g->direct = false;
+        ++g->k;
+    }
+    return WAKE_OK;
+}
+
+}  // namespace
+
+// ==================================================================== C ABI
+extern "C" {
+
+const char* wake_gpu_last_error(void) { return t_err.c_str(); }
+int wake_gpu_last_error_code(void) { return t_code; }
+void wake_gpu_clear_error(void) { clear_error(); }
+const char* wake_gpu_version(void) { return "wake_b200 0.1.0 (sm_100a)"; }
+
+wake_grid* wake_grid_create(int q, int nx, int ny, int nz, float tau, int storage) {
+    if (!(q == 9 || q == 19 || q == 27) || nx < 1 || ny < 1 || nz < 1 || (q == 9 && nz != 1) ||
+        storage < 0 || storage > 2 || !(tau > 0.5f)) {
+        set_error(WAKE_ERR_INVALID, "wake_grid_create: invalid lattice, size, tau or storage");
+        return nullptr;
+    }
+    const long long N = static_cast<long long>(nx) * ny * nz;
+    if (N >= (1ll << 31)) {
+        set_error(WAKE_ERR_INVALID, "wake_grid_create: more than 2^31 - 1 nodes");
+        return nullptr;
+    }
+    auto* g = new wake_grid(q);
+    g->Q = q;
+    g->D = g->lat.D;
+    g->nx = nx;
+    g->ny = ny;
+    g->nz = nz;
+    g->N = N;
+    g->pitch = (N + 63) / 64 * 64;
+    g->storage = storage;
+    g->elem = storage == WAKE_STORE_F32 ? 4 : 2;
+    g->phys.tau = tau;
+    g->phys.lambda_trt = 0.25f;
+    g->phys.tau_bulk = (q == 9) ? 1.63f : (q == 19 ? 1.19f : 1.0f);
+    g->phys.cs_smag = 0.14f;
+    g->phys.s3 = 1.0f;
+    g->phys.s4 = 1.0f;
+    g->phys.mrt_exact = 0;
+    g->types.assign(N, WAKE_CELL_FLUID);
+    g->choose_block(0);
+    cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) g->own_stream = true;
+    const std::size_t sb = g->elem * static_cast<std::size_t>(q) * g->pitch;
+    if (e == cudaSuccess) e = g->A.ensure(sb);
+    if (e == cudaSuccess) e = g->B.ensure(sb);
+    if (e == cudaSuccess) e = g->d_types.ensure(N);
+    if (e == cudaSuccess) e = g->d_flags.ensure(N);
+    if (e == cudaSuccess) e = g->d_status.ensure(sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemsetAsync(g->d_status.p, 0, sizeof(unsigned), g->stream);
+    if (e != cudaSuccess) {
+        set_error(e == cudaErrorMemoryAllocation ? WAKE_ERR_NOMEM : WAKE_ERR_CUDA,
+                  std::string("wake_grid_create: ") + cudaGetErrorString(e));
+        delete g;
+        return nullptr;
+    }
+    if (wake_grid_initialize(g, 1.0f, 0.f, 0.f, 0.f) != WAKE_OK) {
+        delete g;
+        return nullptr;
+    }
+    return g;
+}
+
+void wake_grid_destroy(wake_grid* g) {
+    if (!g) return;
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    delete g;
+}
+
+int wake_grid_set_stream(wake_grid* g, void* stream) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    if (g->own_stream) cudaStreamDestroy(g->stream);
+    g->own_stream = false;
+    if (stream) {
+        g->stream = static_cast<cudaStream_t>(stream);
+    } else {
+        WK_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+        g->own_stream = true;
+    }
+    g->invalidate_graph();
+    return WAKE_OK;
+}
+
+int wake_grid_set_model(wake_grid* g, int collision, int les, float cs_smag, float lambda_trt, float tau_bulk,
+                        int mrt_exact, float s3, float s4) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (collision < 0 || collision > 2 || !(tau_bulk > 0.5f) || !(lambda_trt > 0.f))
+        return set_error(WAKE_ERR_INVALID, "wake_grid_set_model: invalid collision, tau_bulk or lambda");
+    g->collision = collision;
+    g->les = les ? 1 : 0;
+    g->phys.cs_smag = cs_smag;
+    g->phys.lambda_trt = lambda_trt;
+    g->phys.tau_bulk = tau_bulk;
+    g->phys.mrt_exact = mrt_exact ? 1 : 0;
+    g->phys.s3 = s3;
+    g->phys.s4 = s4;
+    g->invalidate_graph();
+    return WAKE_OK;
+}
+
+int wake_grid_set_relaxation_time(wake_grid* g, float tau) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (!(tau > 0.5f)) return set_error(WAKE_ERR_INVALID, "tau must exceed 1/2");
+    g->phys.tau = tau;
+    g->invalidate_graph();
+    return WAKE_OK;
+}
+
+int wake_grid_set_cell_type(wake_grid* g, int x, int y, int z, int type) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    // out-of-range coordinates are ignored, as in LatticeGrid2D::set_cell_type (lattice_grid_2d.cpp:122-126)
+    if (x < 0 || x >= g->nx || y < 0 || y >= g->ny || z < 0 || z >= g->nz) return WAKE_OK;
+    g->types[idx3(g, x, y, z)] = static_cast<uint8_t>(type & FL_TYPE);
+    g->geom_dirty = true;
+    return WAKE_OK;
+}
+
+int wake_grid_set_cell_types(wake_grid* g, const uint8_t* types) {
+    if (!valid_grid(g) || !types) return set_error(WAKE_ERR_INVALID, "null argument");
+    for (long long i = 0; i < g->N; ++i) g->types[i] = types[i] & FL_TYPE;
+    g->geom_dirty = true;
+    return WAKE_OK;
+}
+
+int wake_grid_get_cell_types(wake_grid* g, uint8_t* types) {
+    if (!valid_grid(g) || !types) return set_error(WAKE_ERR_INVALID, "null argument");
+    std::memcpy(types, g->types.data(), g->N);
+    return WAKE_OK;
+}
+
+int wake_grid_set_solid_box(wake_grid* g, int x0, int y0, int z0, int x1, int y1, int z1) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    for (int z = std::max(0, z0); z <= std::min(g->nz - 1, z1); ++z)
+        for (int y = std::max(0, y0); y <= std::min(g->ny - 1, y1); ++y)
+            for (int x = std::max(0, x0); x <= std::min(g->nx - 1, x1); ++x) g->types[idx3(g, x, y, z)] = WAKE_CELL_SOLID;
+    g->geom_dirty = true;
+    return WAKE_OK;
+}
+
+// LatticeGrid2D::set_solid_circle (lattice_grid_2d.cpp:143-158): bounding box
+// truncated with int casts, cell centres at integer coordinates, r^2 test in float.
+int wake_grid_set_solid_circle(wake_grid* g, float cx, float cy, float radius) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    const float r_sq = radius * radius;
+    const int min_x = std::max(0, static_cast<int>(cx - radius - 1));
+    const int max_x = std::min(g->nx - 1, static_cast<int>(cx + radius + 1));
+    const int min_y = std::max(0, static_cast<int>(cy - radius - 1));
+    const int max_y = std::min(g->ny - 1, static_cast<int>(cy + radius + 1));
+    for (int z = 0; z < g->nz; ++z)
+        for (int y = min_y; y <= max_y; ++y)
+            for (int x = min_x; x <= max_x; ++x) {
+                const float dx = static_cast<float>(x) - cx, dy = static_cast<float>(y) - cy;
+                if (dx * dx + dy * dy <= r_sq) g->types[idx3(g, x, y, z)] = WAKE_CELL_SOLID;
+            }
+    g->geom_dirty = true;
+    return WAKE_OK;
+}
+
+// LatticeGrid3D::set_solid_sphere (lattice_grid_3d.cpp:160-182).
+int wake_grid_set_solid_sphere(wake_grid* g, float cx, float cy, float cz, float radius) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    const float r_sq = radius * radius;
+    const int min_x = std::max(0, static_cast<int>(cx - radius - 1));
+    const int max_x = std::min(g->nx - 1, static_cast<int>(cx + radius + 1));
+    const int min_y = std::max(0, static_cast<int>(cy - radius - 1));
+    const int max_y = std::min(g->ny - 1, static_cast<int>(cy + radius + 1));
+    const int min_z = std::max(0, static_cast<int>(cz - radius - 1));
+    const int max_z = std::min(g->nz - 1, static_cast<int>(cz + radius + 1));
+    for (int z = min_z; z <= max_z; ++z)
+        for (int y = min_y; y <= max_y; ++y)
+            for (int x = min_x; x <= max_x; ++x) {
+                const float dx = static_cast<float>(x) - cx, dy = static_cast<float>(y) - cy,
+                            dz = static_cast<float>(z) - cz;
+                if (dx * dx + dy * dy + dz * dz <= r_sq) g->types[idx3(g, x, y, z)] = WAKE_CELL_SOLID;
+            }
+    g->geom_dirty = true;
+    return WAKE_OK;
+}
+
+int wake_grid_set_inflow_west(wake_grid* g, float ux, float uy, float uz) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    g->inflow = 1;
+    g->uin[0] = ux;
+    g->uin[1] = uy;
+    g->uin[2] = uz;
+    for (int z = 0; z < g->nz; ++z)
+        for (int y = 0; y < g->ny; ++y) g->types[idx3(g, 0, y, z)] = WAKE_CELL_INFLOW;
+    g->geom_dirty = true;
+    return WAKE_OK;
+}
+
+int wake_grid_set_outflow_east(wake_grid* g, float rho_out) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (!(rho_out > 0.f)) return set_error(WAKE_ERR_INVALID, "rho_out must be positive");
+    g->outflow = 1;
+    g->rho_out = rho_out;
+    for (int z = 0; z < g->nz; ++z)
+        for (int y = 0; y < g->ny; ++y) g->types[idx3(g, g->nx - 1, y, z)] = WAKE_CELL_OUTFLOW;
+    g->geom_dirty = true;
+    return WAKE_OK;
+}
+
+// 2D: LatticeGrid2D::set_moving_wall_north (lattice_grid_2d.cpp:178-184);
+// 3D: LatticeGrid3D::set_moving_wall_top (lattice_grid_3d.cpp:205-215).
+int wake_grid_set_moving_wall(wake_grid* g, float uw_x, float uw_y, float uw_z) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    g->lid = 1;
+    g->uw[0] = uw_x;
+    g->uw[1] = uw_y;
+    g->uw[2] = uw_z;
+    for (int z = 0; z < g->nz; ++z)
+        for (int x = 0; x < g->nx; ++x) g->types[idx3(g, x, g->ny - 1, z)] = WAKE_CELL_MOVING_WALL;
+    g->geom_dirty = true;
+    return WAKE_OK;
+}
+
+int wake_grid_set_periodic(wake_grid* g, int periodic_y, int periodic_z) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (g->D != 3 && (periodic_y || periodic_z)) return set_error(WAKE_ERR_INVALID, "periodic y/z needs a 3D lattice");
+    g->periodic_y = periodic_y ? 1 : 0;
+    g->periodic_z = periodic_z ? 1 : 0;
+    g->geom_dirty = true;
+    return WAKE_OK;
+}
+
+int wake_grid_set_curved_links(wake_grid* g, int n, const int* fluid_indices, const int* q_dirs, const float* delta,
+                               const float* uw_x, const float* uw_y, const float* uw_z) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (g->Q != 19 && n > 0) return set_error(WAKE_ERR_INVALID, "curved links are D3Q19 only");
+    if (n < 0 || (n > 0 && (!fluid_indices || !q_dirs || !delta)))
+        return set_error(WAKE_ERR_INVALID, "wake_grid_set_curved_links: bad arguments");
+    for (int k = 0; k < n; ++k)
+        if (fluid_indices[k] < 0 || fluid_indices[k] >= g->N || q_dirs[k] < 1 || q_dirs[k] >= g->Q ||
+            !(delta[k] > 0.f))
+            return set_error(WAKE_ERR_INVALID, "wake_grid_set_curved_links: link out of range");
+    g->link_node.assign(fluid_indices, fluid_indices + n);
+    g->link_q.assign(q_dirs, q_dirs + n);
+    g->link_delta.assign(delta, delta + n);
+    g->link_uw.assign(3 * static_cast<std::size_t>(n), 0.f);
+    for (int k = 0; k < n; ++k) {
+        if (uw_x) g->link_uw[3 * k] = uw_x[k];
+        if (uw_y) g->link_uw[3 * k + 1] = uw_y[k];
+        if (uw_z) g->link_uw[3 * k + 2] = uw_z[k];
+    }
+    g->links_dirty = true;
+    g->geom_dirty = true;
+    return WAKE_OK;
+}
+
+// LatticeGrid3D::build_curved_sphere_links (lattice_grid_3d.cpp:217-290): for
+// every Fluid node and direction whose neighbour (x periodic, y/z in range) is
+// Solid, intersect the link with the sphere; delta defaults to 1/2 and is
+// clamped to [0.01, 0.99].
+int wake_grid_build_curved_sphere_links(wake_grid* g, float cx, float cy, float cz, float radius) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (g->Q != 19) return set_error(WAKE_ERR_INVALID, "curved links are D3Q19 only");
+    std::vector<int> idx, qd;
+    std::vector<float> delta;
+    for (int z = 0; z < g->nz; ++z)
+        for (int y = 0; y < g->ny; ++y)
+            for (int x = 0; x < g->nx; ++x) {
+                if (g->types[idx3(g, x, y, z)] != WAKE_CELL_FLUID) continue;
+                for (int q = 1; q < 19; ++q) {
+                    const int xn = (x + g->lat.cx[q] + g->nx) % g->nx, yn = y + g->lat.cy[q], zn = z + g->lat.cz[q];
+                    if (yn < 0 || yn >= g->ny || zn < 0 || zn >= g->nz) continue;
+                    if (g->types[idx3(g, xn, yn, zn)] != WAKE_CELL_SOLID) continue;
+                    const float px = static_cast<float>(x) - cx, py = static_cast<float>(y) - cy,
+                                pz = static_cast<float>(z) - cz;
+                    const float dx = float(g->lat.cx[q]), dy = float(g->lat.cy[q]), dz = float(g->lat.cz[q]);
+                    const float a = dx * dx + dy * dy + dz * dz;
+                    const float b = 2.0f * (px * dx + py * dy + pz * dz);
+                    const float c = (px * px + py * py + pz * pz) - radius * radius;
+                    const float disc = b * b - 4.0f * a * c;
+                    float d = 0.5f;
+                    if (disc >= 0.0f) {
+                        const float t1 = (-b - std::sqrt(disc)) / (2.0f * a);
+                        const float t2 = (-b + std::sqrt(disc)) / (2.0f * a);
+                        if (t1 >= 0.0f && t1 <= 1.0f) d = t1;
+                        else if (t2 >= 0.0f && t2 <= 1.0f) d = t2;
+                    }
+                    d = std::clamp(d, 0.01f, 0.99f);
+                    idx.push_back(static_cast<int>(idx3(g, x, y, z)));
+                    qd.push_back(q);
+                    delta.push_back(d);
+                }
+            }
+    return wake_grid_set_curved_links(g, static_cast<int>(idx.size()), idx.data(), qd.data(), delta.data(), nullptr,
+                                      nullptr, nullptr);
+}
+
+int wake_grid_num_curved_links(wake_grid* g) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    return static_cast<int>(g->link_node.size());
+}
+
+int wake_grid_get_curved_links(wake_grid* g, int* fluid_indices, int* q_dirs, float* delta) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    const std::size_t n = g->link_node.size();
+    if (fluid_indices) std::copy(g->link_node.begin(), g->link_node.end(), fluid_indices);
+    if (q_dirs) std::copy(g->link_q.begin(), g->link_q.end(), q_dirs);
+    if (delta) std::copy(g->link_delta.begin(), g->link_delta.end(), delta);
+    return static_cast<int>(n);
+}
+
+int wake_grid_initialize(wake_grid* g, float rho, float ux, float uy, float uz) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    std::vector<float> f(static_cast<std::size_t>(g->Q) * g->N);
+    float one[27];
+    equilibrium(g->lat, rho, ux, uy, (g->D == 3) ? uz : 0.f, one, 1);
+    for (int q = 0; q < g->Q; ++q) std::fill(f.begin() + q * g->N, f.begin() + (q + 1) * g->N, one[q]);
+    return upload_f0(g, f.data(), cudaMemcpyHostToDevice);
+}
+
+int wake_grid_initialize_fields(wake_grid* g, const float* rho, const float* ux, const float* uy, const float* uz) {
+    if (!valid_grid(g) || !rho || !ux || !uy) return set_error(WAKE_ERR_INVALID, "null field");
+    std::vector<float> f(static_cast<std::size_t>(g->Q) * g->N);
+    for (long long i = 0; i < g->N; ++i)
+        equilibrium(g->lat, rho[i], ux[i], uy[i], (uz && g->D == 3) ? uz[i] : 0.f, f.data() + i, g->N);
+    return upload_f0(g, f.data(), cudaMemcpyHostToDevice);
+}
+
+int wake_grid_set_populations(wake_grid* g, const float* f) {
+    if (!valid_grid(g) || !f) return set_error(WAKE_ERR_INVALID, "null populations");
+    return upload_f0(g, f, cudaMemcpyHostToDevice);
+}
+
+int wake_grid_set_populations_device(wake_grid* g, const float* f_dev) {
+    if (!valid_grid(g) || !f_dev) return set_error(WAKE_ERR_INVALID, "null populations");
+    return upload_f0(g, f_dev, cudaMemcpyDeviceToDevice);
+}
+
+int wake_grid_enable_forces(wake_grid* g, float cx, float cy, float cz, float r_max, int history_capacity) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (history_capacity < 1) return set_error(WAKE_ERR_INVALID, "history capacity must be positive");
+    g->mem_on = 1;
+    g->center[0] = cx;
+    g->center[1] = cy;
+    g->center[2] = (g->D == 3) ? cz : 0.f;
+    g->rmax = r_max;
+    g->hist_cap = history_capacity;
+    WK_CUDA(g->d_hist.ensure(sizeof(double) * 3 * history_capacity));
+    WK_CUDA(g->d_counters.ensure(sizeof(unsigned) * 2));
+    WK_CUDA(cudaMemsetAsync(g->d_counters.p, 0, sizeof(unsigned) * 2, g->stream));
+    WK_CUDA(cudaMemsetAsync(g->d_hist.p, 0, sizeof(double) * 3 * history_capacity, g->stream));
+    // the flags carry the momentum-exchange bit; a pending geometry change
+    // is applied (with its state resync) by the next step instead
+    if (!g->geom_dirty) {
+        const int r = rebuild_flags(g);
+        if (r) return r;
+    }
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    return WAKE_OK;
+}
+
+int wake_grid_disable_forces(wake_grid* g) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    g->mem_on = 0;
+    if (!g->geom_dirty) {
+        const int r = rebuild_flags(g);
+        if (r) return r;
+    }
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    return WAKE_OK;
+}
+
+long long wake_grid_force_count(wake_grid* g) {
+    if (!valid_grid(g) || !g->mem_on) return 0;
+    unsigned c[2] = {0, 0};
+    if (cudaMemcpyAsync(c, g->d_counters.p, sizeof(c), cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
+        cudaStreamSynchronize(g->stream) != cudaSuccess)
+        return set_error(WAKE_ERR_CUDA, "wake_grid_force_count: copy failed");
+    return c[1];
+}
+
+int wake_grid_get_force_history(wake_grid* g, double* out, int max) {
+    if (!valid_grid(g) || !out || max < 0) return set_error(WAKE_ERR_INVALID, "bad arguments");
+    if (!g->mem_on) return 0;
+    const long long count = wake_grid_force_count(g);
+    if (count < 0) return static_cast<int>(count);
+    std::vector<double> ring(3 * static_cast<std::size_t>(g->hist_cap));
+    WK_CUDA(cudaMemcpyAsync(ring.data(), g->d_hist.p, sizeof(double) * ring.size(), cudaMemcpyDeviceToHost, g->stream));
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    const long long first = std::max(0ll, count - g->hist_cap);
+    int n = 0;
+    for (long long s = first; s < count && n < max; ++s, ++n) {
+        const long long slot = s % g->hist_cap;
+        for (int c = 0; c < 3; ++c) out[3 * n + c] = ring[3 * slot + c];
+    }
+    return n;
+}
+
+int wake_grid_step(wake_grid* g, int n, float gx, float gy, float gz) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (n < 0) return set_error(WAKE_ERR_INVALID, "negative step count");
+    int r = prepare(g);
+    if (r) return r;
+    const float gnew[3] = {gx, gy, (g->D == 3) ? gz : 0.f};
+    if (gnew[0] != g->phys.g[0] || gnew[1] != g->phys.g[1] || gnew[2] != g->phys.g[2]) g->invalidate_graph();
+    for (int a = 0; a < 3; ++a) g->phys.g[a] = gnew[a];
+    int done = 0;
+    if (g->graph_steps > 0 && n >= g->graph_steps) {
+        // (re)capture a graph of graph_steps launches from the current parity
+        const int gs = g->graph_steps;
+        if (!g->graph_ok || g->graph_cur != g->cur) {
+            if (g->graph) {
+                cudaGraphExecDestroy(g->graph);
+                g->graph = nullptr;
+            }
+            const int cur0 = g->cur;
+            const long long k0 = g->k;
+            cudaGraph_t graph = nullptr;
+            WK_CUDA(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+            r = do_steps(g, gs);
+            cudaError_t e = cudaStreamEndCapture(g->stream, &graph);
+            g->cur = cur0;
+            g->k = k0;
+            if (r) return r;
+            if (e != cudaSuccess) return set_error(WAKE_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&g->graph, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return set_error(WAKE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            g->graph_cur = cur0;
+            g->graph_ok = true;
+        }
+        while (n - done >= gs && g->cur == g->graph_cur) {
+            WK_CUDA(cudaGraphLaunch(g->graph, g->stream));
+            g->k += gs;
+            g->direct = false;
+            done += gs;
+        }
+    }
+    return do_steps(g, n - done);
+}
+
+int wake_grid_use_graph(wake_grid* g, int steps_per_graph) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (steps_per_graph < 0) return set_error(WAKE_ERR_INVALID, "negative graph size");
+    // an even count returns to the same buffer parity, so one graph serves every replay
+    g->graph_steps = steps_per_graph > 0 && steps_per_graph % 2 ? steps_per_graph + 1 : steps_per_graph;
+    g->invalidate_graph();
+    return WAKE_OK;
+}
+
+long long wake_grid_step_count(wake_grid* g) { return g ? g->k : -1; }
+
+int wake_grid_synchronize(wake_grid* g) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    unsigned st = 0;
+    WK_CUDA(cudaMemcpy(&st, g->d_status.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (st & ERR_NONFINITE) return set_error(WAKE_ERR_NUMERIC, "non-finite or non-positive density on the device");
+    return WAKE_OK;
+}
+
+int wake_grid_get_populations(wake_grid* g, float* f) {
+    if (!valid_grid(g) || !f) return set_error(WAKE_ERR_INVALID, "null output");
+    int r = prepare(g);
+    if (r) return r;
+    r = materialise(g, true, false);
+    if (r) return r;
+    WK_CUDA(cudaMemcpy2DAsync(f, sizeof(float) * g->N, g->m_f.p, sizeof(float) * g->pitch, sizeof(float) * g->N, g->Q,
+                              cudaMemcpyDefault, g->stream));
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    return WAKE_OK;
+}
+
+int wake_grid_get_macroscopic(wake_grid* g, float* rho, float* ux, float* uy, float* uz, float* speed) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    int r = prepare(g);
+    if (r) return r;
+    r = materialise(g, false, true);
+    if (r) return r;
+    const std::size_t b = sizeof(float) * g->N;
+    if (rho) WK_CUDA(cudaMemcpyAsync(rho, g->m_rho.p, b, cudaMemcpyDefault, g->stream));
+    if (ux) WK_CUDA(cudaMemcpyAsync(ux, g->m_ux.p, b, cudaMemcpyDefault, g->stream));
+    if (uy) WK_CUDA(cudaMemcpyAsync(uy, g->m_uy.p, b, cudaMemcpyDefault, g->stream));
+    if (uz) WK_CUDA(cudaMemcpyAsync(uz, g->m_uz.p, b, cudaMemcpyDefault, g->stream));
+    if (speed) WK_CUDA(cudaMemcpyAsync(speed, g->m_speed.p, b, cudaMemcpyDefault, g->stream));
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    return WAKE_OK;
+}
+
+static int diag_all(wake_grid* g, double out[4]) {
+    int r = prepare(g);
+    if (r) return r;
+    r = materialise(g, false, true);
+    if (r) return r;
+    const int nb = 592;  // 4 x 148 SMs
+    WK_CUDA(g->m_diag.ensure(sizeof(double) * 4 * nb));
+    k_diag_partials<<<nb, 256, 0, g->stream>>>(g->m_rho.as<float>(), g->m_speed.as<float>(), g->d_flags.as<uint8_t>(),
+                                                g->N, g->m_diag.as<double>());
+    WK_CUDA(cudaGetLastError());
+    std::vector<double> h(4 * nb);
+    WK_CUDA(cudaMemcpyAsync(h.data(), g->m_diag.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, g->stream));
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    out[0] = out[1] = out[2] = out[3] = 0.0;
+    for (int b = 0; b < nb; ++b) {
+        out[0] += h[4 * b];
+        out[1] += h[4 * b + 1];
+        out[2] = std::max(out[2], h[4 * b + 2]);
+        out[3] += h[4 * b + 3];
+    }
+    return WAKE_OK;
+}
+
+int wake_grid_diagnostics(wake_grid* g, double* total_mass, double* kinetic_energy, double* max_speed) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    double d[4];
+    const int r = diag_all(g, d);
+    if (r) return r;
+    if (total_mass) *total_mass = d[0];
+    if (kinetic_energy) *kinetic_energy = d[1];
+    if (max_speed) *max_speed = d[2];
+    return WAKE_OK;
+}
+
+int wake_grid_total_mass(wake_grid* g, double* mass) {
+    if (!valid_grid(g) || !mass) return set_error(WAKE_ERR_INVALID, "null output");
+    double d[4];
+    const int r = diag_all(g, d);
+    if (r) return r;
+    *mass = d[3];
+    return WAKE_OK;
+}
+
+int wake_grid_info(wake_grid* g, int* q, int* nx, int* ny, int* nz, int* storage, long long* pitch) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (q) *q = g->Q;
+    if (nx) *nx = g->nx;
+    if (ny) *ny = g->ny;
+    if (nz) *nz = g->nz;
+    if (storage) *storage = g->storage;
+    if (pitch) *pitch = g->pitch;
+    return WAKE_OK;
+}
+
+void* wake_grid_state_buffer(wake_grid* g, int which) {
+    if (!g) return nullptr;
+    return g->buf(which == 0 ? g->cur : 1 - g->cur);
+}
+
+int wake_grid_set_block(wake_grid* g, int threads_per_block) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (threads_per_block < 32 || threads_per_block > 512 || threads_per_block % 32)
+        return set_error(WAKE_ERR_INVALID, "threads per block must be a multiple of 32 in [32, 512]");
+    g->choose_block(threads_per_block);
+    g->geom_dirty = true;  // momentum-exchange block slots depend on the launch shape
+    return WAKE_OK;
+}
+
+int wake_grid_get_block(wake_grid* g) { return g ? g->tpb : WAKE_ERR_INVALID; }
+
+}  // extern "C"

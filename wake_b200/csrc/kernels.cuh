@@ -1,0 +1,46 @@
+// Launch interface between the host engine and the per-lattice kernel
+// translation units (kernels_q9.cu, kernels_q19.cu, kernels_q27.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "stream_collide.cuh"
+
+namespace wk {
+
+struct Launch {
+    int tpb;       // threads per block (one thread per node along x)
+    int xchunks;   // blocks per row
+    int rows;      // ny * nz
+    cudaStream_t stream;
+};
+
+struct FlagCfg {
+    int zh_rule;         // 0 none, 1: 2D reference rule (columns x=0 / x=nx-1, rows 1..ny-2), 2: typed faces
+    int inflow, outflow;
+    int mem_enabled;
+    float center[3];
+    float r_max, r_max_sq;
+};
+
+// Per-lattice entry points (defined once per Q in kernels_impl.cuh).
+#define WK_DECLARE_LAUNCHERS(Q)                                                                                   \
+    cudaError_t launch_step_q##Q(int coll, int store, bool les, const StepArgs& a, const Launch& L);             \
+    cudaError_t launch_materialise_q##Q(int store, const void* fin, const uint8_t* flags, const Geo& geo,        \
+                                        const Links& links, const Physics& phys, const Out& out,                 \
+                                        const Launch& L, int direct);                                            \
+    cudaError_t launch_initial_q##Q(int coll, int store, bool les, const float* f0, void* a, void* b,            \
+                                    const uint8_t* flags, const Geo& geo, const Physics& phys, const Launch& L); \
+    cudaError_t launch_flags_q##Q(const uint8_t* types, uint8_t* flags, const Geo& geo, const FlagCfg& cfg,      \
+                                  const Launch& L);                                                              \
+    cudaError_t launch_block_marks_q##Q(const uint8_t* flags, int* marks, const Geo& geo, const Launch& L);
+
+WK_DECLARE_LAUNCHERS(9)
+WK_DECLARE_LAUNCHERS(19)
+WK_DECLARE_LAUNCHERS(27)
+
+// Marks FL_BFL on link nodes (clearing FL_FAST) and records each node's first link.
+cudaError_t launch_link_marks(const int* link_node, int n_links, uint8_t* flags, int* node_start,
+                              cudaStream_t stream);
+
+}  // namespace wk

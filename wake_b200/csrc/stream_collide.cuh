@@ -1,0 +1,341 @@
+// Fused pull-stream + boundary + moments + momentum-exchange + collide kernels.
+//
+// State between steps is the POST-collision population buffer g^k (A/B
+// ping-pong, SoA planes [q][node], plane pitch a multiple of 64 elements).
+// The reference keeps the post-stream, pre-collision f^k instead
+// (src/grid/lattice_grid_2d.cpp:195-265): f^{k+1} = ZouHe(BFL(Stream(Collide(f^k)))).
+// With g^k = Collide(f^k), one fused launch computes, per node,
+//
+//   f^{k+1}(x) = ZouHe(BFL(Pull(g^k)))(x)      -- reference steps 3-5
+//   rho, u, momentum exchange from f^{k+1}(x)   -- reference step 6 + scenario MEM
+//   g^{k+1}(x) = Collide(f^{k+1}(x))            -- next step's collide
+//
+// so every quantity the reference exposes after k steps is available from
+// g^{k-1} (re-gathered by the materialise kernel), and one step moves
+// 2*Q*sizeof(pop) + 1 flag byte per node through HBM.
+#pragma once
+
+#include "lattice.cuh"
+
+namespace wk {
+
+// Device-side error word bits (read by the host after a launch sequence).
+enum : unsigned { ERR_NONFINITE = 1u, ERR_BAD_CONFIG = 2u };
+
+struct Geo {
+    int nx, ny, nz;
+    int periodic_y, periodic_z;   // 3D: wrap y / z instead of half-way bounce-back walls
+    long long pitch;              // elements per population plane
+    float uin[3];                 // Zou-He inlet velocity
+    float rho_out;                // Zou-He outlet density
+    float mom[27];                // moving-wall term 2 w_q 3 (c_q . u_w) (d2q9_streaming.ispc:49-53)
+};
+
+struct Links {                    // curved-boundary (BFL) links sorted by fluid node
+    const int* node_start;        // [N] first link of the node, read only where FL_BFL is set
+    const int* node;              // [n] fluid node index
+    const int* q;                 // [n] direction pointing into the solid
+    const float* delta;           // [n] wall distance fraction
+    const float* mom;             // [n] moving-wall term of the branch taken (d3q19_curved.ispc:57,62)
+    int count;
+};
+
+struct MemCfg {                   // momentum-exchange monitor
+    int enabled;
+    float center[3];
+    float r_max, r_max_sq;
+    const int* block_slot;        // [grid] slot of the block's partial, -1 if none
+    double* partial;              // [n_slots][3]
+    unsigned* arrivals;           // block arrival counter (reset by the last block)
+    unsigned* hist_step;          // number of entries written so far
+    double* hist;                 // [hist_cap][3]: (Fx, Fy, Tz) in 2D, (Fx, Fy, Fz) in 3D
+    int hist_cap;
+    int n_slots;
+};
+
+struct Out {                      // optional outputs of the materialise kernel
+    float* f;                     // FP32 f^k planes (pitch as the state buffers)
+    float* rho;
+    float* ux;
+    float* uy;
+    float* uz;
+    float* speed;
+};
+
+template <int Q>
+__device__ __forceinline__ int wrap(int v, int n) {
+    v += (v < 0) ? n : 0;
+    v -= (v >= n) ? n : 0;
+    return v;
+}
+
+// Pull f^{k+1}(x) out of g^k. `bb` gets bit q when the pull of q bounced off a
+// solid or moving-wall node (in range), which marks the momentum-exchange link
+// (x, opp(q)).
+template <int Q, int S>
+__device__ __forceinline__ void gather(const typename Codec<S>::T* __restrict__ fin, const Geo& G,
+                                       const uint8_t* __restrict__ flags, const Links& B, int x, int y, int z,
+                                       long long i, uint8_t fl, float f[Q], unsigned& bb) {
+    using L = Lat<Q>;
+    using C = Codec<S>;
+    const long long P = G.pitch;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    bb = 0u;
+    if (fl & FL_FAST) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int sx = L::cx(q) ? wrap<Q>(x - L::cx(q), nx) : x;
+            int sy = y - L::cy(q), sz = z - L::cz(q);
+            if (L::cy(q) && G.periodic_y) sy = wrap<Q>(sy, ny);
+            if (L::cz(q) && G.periodic_z) sz = wrap<Q>(sz, nz);
+            const long long s = (static_cast<long long>(sz) * ny + sy) * nx + sx;
+            f[q] = C::load(fin + q * P + s, L::w(q));
+        }
+        return;
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int o = L::opp(q);
+        const int sx = L::cx(q) ? wrap<Q>(x - L::cx(q), nx) : x;
+        int sy = y - L::cy(q), sz = z - L::cz(q);
+        if (L::cy(q) && G.periodic_y) sy = wrap<Q>(sy, ny);
+        if (L::cz(q) && G.periodic_z) sz = wrap<Q>(sz, nz);
+        const bool inr = (sy >= 0) && (sy < ny) && (sz >= 0) && (sz < nz);
+        if (!inr) {
+            f[q] = C::load(fin + o * P + i, L::w(o));  // domain wall: half-way bounce-back
+            continue;
+        }
+        const long long s = (static_cast<long long>(sz) * ny + sy) * nx + sx;
+        const uint8_t t = flags[s] & FL_TYPE;
+        if (t == CT_SOLID) {
+            f[q] = C::load(fin + o * P + i, L::w(o));
+            bb |= 1u << q;
+        } else if (t == CT_MOVING_WALL) {
+            f[q] = C::load(fin + o * P + i, L::w(o)) + G.mom[q];
+            bb |= 1u << q;
+        } else {
+            f[q] = C::load(fin + q * P + s, L::w(q));
+        }
+    }
+    if constexpr (Q == 19) {
+        if (fl & FL_BFL) {
+            // Bouzidi linear interpolation from post-collision values (d3q19_curved.ispc:36-68).
+            for (int k = B.node_start[i]; k < B.count && B.node[k] == i; ++k) {
+                const int q = B.q[k];
+                int qcx, qcy, qcz, o;
+                float wq;
+                rt_dir<19>(q, qcx, qcy, qcz, o, wq);
+                const float delta = B.delta[k];
+                const float fi = C::load(fin + q * P + i, wq);
+                float val;
+                if (delta < 0.5f) {
+                    const int xff = wrap<Q>(x - qcx, nx);
+                    const int yff = y - qcy, zff = z - qcz;
+                    float fff = fi;
+                    if (yff >= 0 && yff < ny && zff >= 0 && zff < nz) {
+                        const long long s = (static_cast<long long>(zff) * ny + yff) * nx + xff;
+                        fff = C::load(fin + q * P + s, wq);
+                    }
+                    val = 2.0f * delta * fi + (1.0f - 2.0f * delta) * fff - B.mom[k];
+                } else {
+                    const float fo = C::load(fin + o * P + i, rt_w19(o));
+                    const float i2d = 1.0f / (2.0f * delta);
+                    val = i2d * fi + (1.0f - i2d) * fo - B.mom[k];
+                }
+#pragma unroll
+                for (int qq = 0; qq < Q; ++qq)
+                    if (qq == o) f[qq] = val;
+            }
+        }
+    }
+    if (fl & FL_ZH_IN) zou_he_inlet<Q>(f, G.uin);
+    if (fl & FL_ZH_OUT) zou_he_outlet<Q>(f, G.rho_out);
+}
+
+// Momentum-exchange contributions of one fluid node (forces_momentum_exchange.ispc:33-63):
+// links (x, q) with a Solid / MovingWall node at x + c_q (x periodic, y/z in range)
+// within r_max of the centre; F += 2 f_q c_q, torque from r x F in 2D.
+template <int Q>
+__device__ __forceinline__ void mem_node(const float* f, unsigned bb, int x, int y, int z, const Geo& G,
+                                         const MemCfg& M, double acc[3]) {
+    using L = Lat<Q>;
+#pragma unroll
+    for (int q = 1; q < Q; ++q) {
+        if (!(bb & (1u << L::opp(q)))) continue;
+        const int yn = y + L::cy(q), zn = z + L::cz(q);
+        if (yn < 0 || yn >= G.ny || zn < 0 || zn >= G.nz) continue;
+        // same float roundings as the reference's filter: no contraction
+        const float rx = __fsub_rn(__fadd_rn(float(x), 0.5f * float(L::cx(q))), M.center[0]);
+        const float ry = __fsub_rn(__fadd_rn(float(y), 0.5f * float(L::cy(q))), M.center[1]);
+        const float rz = __fsub_rn(__fadd_rn(float(z), 0.5f * float(L::cz(q))), M.center[2]);
+        float r2 = __fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry));
+        if (L::D == 3) r2 = __fadd_rn(r2, __fmul_rn(rz, rz));
+        if (!(M.r_max <= 0.0f || r2 <= M.r_max_sq)) continue;
+        const double fv = f[q];
+        const double dfx = 2.0 * fv * L::cx(q), dfy = 2.0 * fv * L::cy(q);
+        acc[0] += dfx;
+        acc[1] += dfy;
+        if (L::D == 2) acc[2] += double(rx) * dfy - double(ry) * dfx;
+        else acc[2] += 2.0 * fv * L::cz(q);
+    }
+}
+
+// Deterministic block reduction of the momentum exchange: each contributing block
+// writes its partial to a fixed slot; the last block to arrive sums the slots in
+// slot order and appends the step's force to the history. No waiting: arrival is
+// counted with one atomic, the last arriver does the final sum.
+__device__ __forceinline__ void mem_block_finish(const MemCfg& M, double acc[3], int slot) {
+    __shared__ double red[3][32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double v = acc[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[c][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s[3] = {0.0, 0.0, 0.0};
+        for (int w = 0; w < nw; ++w)
+            for (int c = 0; c < 3; ++c) s[c] += red[c][w];
+        for (int c = 0; c < 3; ++c) M.partial[3 * slot + c] = s[c];
+        __threadfence();
+        const unsigned prev = atomicAdd(M.arrivals, 1u);
+        last = (prev == static_cast<unsigned>(M.n_slots) - 1u);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double s[3] = {0.0, 0.0, 0.0};
+        const volatile double* p = M.partial;
+        for (int k = 0; k < M.n_slots; ++k)
+            for (int c = 0; c < 3; ++c) s[c] += p[3 * k + c];
+        const unsigned step = *M.hist_step;
+        double* h = M.hist + 3 * static_cast<long long>(step % static_cast<unsigned>(M.hist_cap));
+        h[0] = s[0];
+        h[1] = s[1];
+        h[2] = s[2];
+        *M.hist_step = step + 1u;
+        *M.arrivals = 0u;
+    }
+}
+
+struct StepArgs {
+    const void* fin;
+    void* fout;
+    const uint8_t* flags;
+    unsigned* status;
+    Geo geo;
+    Links links;
+    MemCfg mem;
+    Physics phys;
+    int xchunks;
+};
+
+// One fused time step: g^{k+1} = Collide(ZouHe(BFL(Pull(g^k)))). Solid nodes are not
+// touched: both buffers hold their frozen populations.
+template <int Q, int COLL, int S, bool LES>
+__global__ void __launch_bounds__(512) k_step(const StepArgs a) {
+    using L = Lat<Q>;
+    using C = Codec<S>;
+    using T = typename C::T;
+    const int row = blockIdx.x / a.xchunks;
+    const int x = (blockIdx.x - row * a.xchunks) * blockDim.x + threadIdx.x;
+    const int ny = a.geo.ny;
+    const int y = row % ny, z = row / ny;
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (x < a.geo.nx) {
+        const long long i = static_cast<long long>(row) * a.geo.nx + x;
+        const uint8_t fl = a.flags[i];
+        if ((fl & FL_TYPE) != CT_SOLID) {
+            float f[Q];
+            unsigned bb;
+            gather<Q, S>(static_cast<const T*>(a.fin), a.geo, a.flags, a.links, x, y, z, i, fl, f, bb);
+            float rho, u[3];
+            node_moments<Q>(f, a.phys.g, rho, u);
+            if (fl & FL_MEM) mem_node<Q>(f, bb, x, y, z, a.geo, a.mem, acc);
+            if (!(rho > 0.0f) || !(fabsf(u[0]) < 1e30f)) atomicOr(a.status, ERR_NONFINITE);
+            collide<Q, COLL, LES>(f, rho, u, a.phys);
+            T* out = static_cast<T*>(a.fout);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) C::store(out + q * a.geo.pitch + i, f[q], L::w(q));
+        }
+    }
+    if (a.mem.enabled) {
+        const int slot = a.mem.block_slot[blockIdx.x];
+        if (slot >= 0) mem_block_finish(a.mem, acc, slot);
+    }
+}
+
+// Re-gather f^k from g^{k-1} and write FP32 populations and/or macroscopic fields
+// (the reference's f_src and its rho/u/speed arrays after step k,
+// lattice_grid_2d.cpp:257-262). Solid nodes report their frozen populations.
+template <int Q, int S>
+__global__ void __launch_bounds__(512) k_materialise(const void* fin_v, const uint8_t* flags, Geo geo, Links links,
+                                                     Physics phys, Out out, int xchunks) {
+    using L = Lat<Q>;
+    using C = Codec<S>;
+    using T = typename C::T;
+    const T* fin = static_cast<const T*>(fin_v);
+    const int row = blockIdx.x / xchunks;
+    const int x = (blockIdx.x - row * xchunks) * blockDim.x + threadIdx.x;
+    if (x >= geo.nx) return;
+    const int y = row % geo.ny, z = row / geo.ny;
+    const long long i = static_cast<long long>(row) * geo.nx + x;
+    const uint8_t fl = flags[i];
+    float f[Q];
+    if ((fl & FL_TYPE) == CT_SOLID) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) f[q] = C::load(fin + q * geo.pitch + i, L::w(q));
+    } else {
+        unsigned bb;
+        gather<Q, S>(fin, geo, flags, links, x, y, z, i, fl, f, bb);
+    }
+    if (out.f) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) out.f[q * geo.pitch + i] = f[q];
+    }
+    if (out.rho) {
+        float rho, u[3];
+        node_moments<Q>(f, phys.g, rho, u);
+        out.rho[i] = rho;
+        out.ux[i] = u[0];
+        out.uy[i] = u[1];
+        if (out.uz) out.uz[i] = u[2];
+        out.speed[i] = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    }
+}
+
+// Initial collide from FP32 populations f^0: buffer A <- g^0 = Collide(f^0)
+// (solid nodes copy through, d2q9_collision_bgk.ispc:22-28), buffer B <- f^0.
+// B's fluid entries are overwritten by the first step; until then B is the
+// reference's f_src, and its solid entries stay the frozen populations.
+template <int Q, int COLL, int S, bool LES>
+__global__ void __launch_bounds__(512) k_initial(const float* f0, void* a_v, void* b_v, const uint8_t* flags,
+                                                 Geo geo, Physics phys, int xchunks) {
+    using L = Lat<Q>;
+    using C = Codec<S>;
+    using T = typename C::T;
+    const int row = blockIdx.x / xchunks;
+    const int x = (blockIdx.x - row * xchunks) * blockDim.x + threadIdx.x;
+    if (x >= geo.nx) return;
+    const long long i = static_cast<long long>(row) * geo.nx + x;
+    float f[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) f[q] = f0[q * geo.pitch + i];
+    T* A = static_cast<T*>(a_v);
+    T* Bf = static_cast<T*>(b_v);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) C::store(Bf + q * geo.pitch + i, f[q], L::w(q));
+    if ((flags[i] & FL_TYPE) != CT_SOLID) {
+        float rho, u[3];
+        node_moments<Q>(f, phys.g, rho, u);
+        collide<Q, COLL, LES>(f, rho, u, phys);
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) C::store(A + q * geo.pitch + i, f[q], L::w(q));
+}
+
+}  // namespace wk

@@ -1,0 +1,201 @@
+"""Seeded synthetic workloads of the benchmark configurations.
+
+All random numbers come from SplitMix64 (Steele, Lea & Flood, "Fast splittable
+pseudorandom number generators", OOPSLA 2014), counter-based so any slice can
+be regenerated, turned into 24-bit uniform floats. Base seed 20261203; domain
+``d`` of a workload uses seed base + d. The same arrays feed the GPU engine,
+the CPU oracle and the reference, so all three start from identical bytes.
+
+Scenario layouts follow the reference scenarios they are modelled on:
+cylinder channel = KarmanVortexScenario::setup (src/scenarios/karman_vortex.cpp:62-88),
+sphere = Sphere3DWakeScenario::setup (src/scenarios/sphere_3d_wake.cpp:64-78),
+Taylor-Green = tests/validation/test_taylor_green_decay.cpp:22-33.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+BASE_SEED = 20261203
+_GAMMA = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+FLUID, SOLID, INFLOW, OUTFLOW, MOVING_WALL = 0, 1, 2, 3, 6
+
+
+def splitmix64(seed: int, n: int, offset: int = 0) -> np.ndarray:
+    """Outputs offset+1 .. offset+n of the SplitMix64 stream of ``seed``."""
+    with np.errstate(over="ignore"):
+        i = np.arange(offset + 1, offset + n + 1, dtype=np.uint64)
+        z = np.uint64(seed % (1 << 64)) + i * _GAMMA
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        return z ^ (z >> np.uint64(31))
+
+
+def uniform24(seed: int, n: int, offset: int = 0) -> np.ndarray:
+    """n floats in [0, 1) with 24 random bits each."""
+    return (splitmix64(seed, n, offset) >> np.uint64(40)).astype(np.float32) * np.float32(2.0**-24)
+
+
+@dataclass
+class Case:
+    """One lattice with geometry, initial fields and run parameters."""
+
+    q: int
+    nx: int
+    ny: int
+    nz: int
+    types: np.ndarray          # uint8 [N]
+    rho: np.ndarray            # float32 [N]
+    ux: np.ndarray
+    uy: np.ndarray
+    uz: np.ndarray
+    tau: float
+    collision: int
+    les: bool = False
+    cs_smag: float = 0.14
+    inflow: tuple | None = None      # (ux, uy, uz) Zou-He inlet
+    outflow: float | None = None     # rho_out
+    periodic_y: bool = False
+    periodic_z: bool = False
+    sphere: tuple | None = None      # (cx, cy, cz, R) for curved links
+    mem: tuple | None = None         # (cx, cy, cz, r_max)
+    ref_area: float = 1.0            # force coefficient area (D in 2D, pi R^2 in 3D)
+    u_ref: float = 0.05
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def n(self) -> int:
+        return self.nx * self.ny * self.nz
+
+
+def cylinder_channel(nx=400, ny=160, diameter=20.0, cx=80.0, cy=80.0, u_in=0.05, tau=0.56, collision=0,
+                     noise=1e-4, seed=BASE_SEED) -> Case:
+    """2D channel: Zou-He inlet/outlet, solid rows y=0 and y=ny-1, solid disk.
+
+    Cell types are set in the order of KarmanVortexScenario::setup: inlet
+    column, outlet column, wall rows, then the disk (LatticeGrid2D::set_solid_circle).
+    """
+    t = np.zeros((ny, nx), np.uint8)
+    t[:, 0] = INFLOW
+    t[:, nx - 1] = OUTFLOW
+    t[0, :] = SOLID
+    t[ny - 1, :] = SOLID
+    _rasterize_circle(t, cx, cy, diameter * 0.5)
+    n = nx * ny
+    r = uniform24(seed, 2 * n)
+    ux = np.float32(u_in) + np.float32(noise) * (np.float32(2.0) * r[:n] - np.float32(1.0))
+    uy = np.float32(noise) * (np.float32(2.0) * r[n:] - np.float32(1.0))
+    return Case(q=9, nx=nx, ny=ny, nz=1, types=t.ravel(), rho=np.ones(n, np.float32), ux=ux.astype(np.float32),
+                uy=uy.astype(np.float32), uz=np.zeros(n, np.float32), tau=tau, collision=collision,
+                inflow=(u_in, 0.0, 0.0), outflow=1.0, mem=(cx, cy, 0.0, 1.5 * diameter), ref_area=diameter,
+                u_ref=u_in)
+
+
+def _rasterize_circle(t: np.ndarray, cx: float, cy: float, radius: float) -> None:
+    """LatticeGrid2D::set_solid_circle (src/grid/lattice_grid_2d.cpp:143-158) in float32."""
+    ny, nx = t.shape
+    f32 = np.float32
+    r_sq = f32(radius) * f32(radius)
+    min_x = max(0, int(f32(cx) - f32(radius) - f32(1)))
+    max_x = min(nx - 1, int(f32(cx) + f32(radius) + f32(1)))
+    min_y = max(0, int(f32(cy) - f32(radius) - f32(1)))
+    max_y = min(ny - 1, int(f32(cy) + f32(radius) + f32(1)))
+    for y in range(min_y, max_y + 1):
+        for x in range(min_x, max_x + 1):
+            dx = f32(x) - f32(cx)
+            dy = f32(y) - f32(cy)
+            if dx * dx + dy * dy <= r_sq:
+                t[y, x] = SOLID
+
+
+def sphere_channel(nx=256, ny=128, nz=128, radius=12.0, center=(64.0, 64.0, 64.0), u_in=0.05, tau=0.52,
+                   collision=1, les=True, cs_smag=0.17, reference_variant=False) -> Case:
+    """3D sphere in a channel.
+
+    Default: Zou-He inlet u_in on x=0, outlet rho=1 on x=nx-1, periodic y/z,
+    TRT + Smagorinsky. ``reference_variant`` gives the form the reference can
+    express: x-periodic, y/z half-way walls, no Zou-He, LES not applied.
+    """
+    t = np.zeros((nz, ny, nx), np.uint8)
+    cx, cy, cz = center
+    _rasterize_sphere(t, cx, cy, cz, radius)
+    inflow = outflow = None
+    if not reference_variant:
+        t[:, :, 0] = np.where(t[:, :, 0] == SOLID, SOLID, INFLOW)
+        t[:, :, nx - 1] = np.where(t[:, :, nx - 1] == SOLID, SOLID, OUTFLOW)
+        inflow, outflow = (u_in, 0.0, 0.0), 1.0
+    n = nx * ny * nz
+    return Case(q=19, nx=nx, ny=ny, nz=nz, types=t.ravel(), rho=np.ones(n, np.float32),
+                ux=np.full(n, u_in, np.float32), uy=np.zeros(n, np.float32), uz=np.zeros(n, np.float32), tau=tau,
+                collision=collision, les=les and not reference_variant, cs_smag=cs_smag, inflow=inflow,
+                outflow=outflow, periodic_y=not reference_variant, periodic_z=not reference_variant,
+                sphere=(cx, cy, cz, radius), mem=(cx, cy, cz, 2.0 * radius), ref_area=math.pi * radius * radius,
+                u_ref=u_in)
+
+
+def _rasterize_sphere(t: np.ndarray, cx, cy, cz, radius) -> None:
+    """LatticeGrid3D::set_solid_sphere (src/grid/lattice_grid_3d.cpp:160-182) in float32."""
+    nz, ny, nx = t.shape
+    f32 = np.float32
+    r_sq = f32(radius) * f32(radius)
+    lo = [max(0, int(f32(c) - f32(radius) - f32(1))) for c in (cx, cy, cz)]
+    hi = [min(m - 1, int(f32(c) + f32(radius) + f32(1))) for c, m in ((cx, nx), (cy, ny), (cz, nz))]
+    zs = np.arange(lo[2], hi[2] + 1)
+    ys = np.arange(lo[1], hi[1] + 1)
+    xs = np.arange(lo[0], hi[0] + 1)
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    dx = X.astype(f32) - f32(cx)
+    dy = Y.astype(f32) - f32(cy)
+    dz = Z.astype(f32) - f32(cz)
+    inside = (dx * dx + dy * dy + dz * dz) <= r_sq
+    sub = t[lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1]
+    sub[inside] = SOLID
+
+
+def taylor_green(L=384, u0=0.04, tau=0.51, q=27, collision=2) -> Case:
+    """Periodic Taylor-Green vortex (form of tests/validation/test_taylor_green_decay.cpp:22-33)."""
+    k = 2.0 * math.pi / L
+    x = np.arange(L, dtype=np.float64)
+    sx, cx_ = np.sin(k * x), np.cos(k * x)
+    c2 = np.cos(2 * k * x)
+    # broadcast over (z, y, x)
+    ux = (u0 * sx[None, None, :] * cx_[None, :, None] * cx_[:, None, None]).astype(np.float32)
+    uy = (-u0 * cx_[None, None, :] * sx[None, :, None] * cx_[:, None, None]).astype(np.float32)
+    p = (u0 * u0 / 16.0) * (c2[None, None, :] + c2[None, :, None]) * (c2[:, None, None] + 2.0)
+    rho = (1.0 + 3.0 * p).astype(np.float32)
+    n = L ** 3
+    return Case(q=q, nx=L, ny=L, nz=L, types=np.zeros(n, np.uint8), rho=rho.ravel(), ux=ux.ravel(), uy=uy.ravel(),
+                uz=np.zeros(n, np.float32), tau=tau, collision=collision, periodic_y=True, periodic_z=True,
+                u_ref=u0, extra={"u0": u0, "k": k})
+
+
+def build_grid(case: Case, storage: str = "f32", les_applies: bool = True):
+    """Configure a wake_b200 grid for a case (initial state = equilibrium of the fields)."""
+    import wake_b200 as wb
+
+    if case.q == 9:
+        g = wb.LatticeGrid2D(case.nx, case.ny, case.tau, storage=storage, les_applies=les_applies)
+    elif case.q == 19:
+        g = wb.LatticeGrid3D(case.nx, case.ny, case.nz, case.tau, storage=storage, les_applies=les_applies)
+    else:
+        g = wb.LatticeGrid3DQ27(case.nx, case.ny, case.nz, case.tau, storage=storage, les_applies=les_applies)
+    g.initialize_fields(case.rho, case.ux, case.uy, case.uz if case.q != 9 else None)
+    g.set_cell_types(case.types)
+    if case.q != 9 and (case.periodic_y or case.periodic_z):
+        g.set_periodic_axes(case.periodic_y, case.periodic_z)
+    if case.inflow is not None:
+        wb.check(wb.lib.wake_grid_set_inflow_west(g.handle, *case.inflow))
+        g.set_cell_types(case.types)  # keep the case's exact typing of the faces
+    if case.outflow is not None:
+        g.set_outflow_east(case.outflow)
+        g.set_cell_types(case.types)
+    if case.sphere is not None and case.q == 19:
+        g.build_curved_sphere_links(*case.sphere)
+    if case.mem is not None:
+        g.enable_forces(*case.mem)
+    return g
