@@ -161,7 +161,7 @@ def allmax(world, v):
 def timed_steps(g, case, steps, warmup, world):
     import torch
 
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # a real stream handle: the legacy default stream is 0
     g.set_stream(stream.cuda_stream)
     g.step(case.collision, use_les=case.les, smag_const=case.cs_smag, n=warmup)
     torch.cuda.synchronize()

@@ -87,5 +87,42 @@ def build(verbose: bool = False) -> Path:
     return so
 
 
+# The reference's own test programs for this path (tests/CMakeLists.txt:20-26), linked
+# against libwake_b200.so instead of the ISPC kernel library.
+REFERENCE_TESTS = [
+    "unit/test_d2q9_moments.cpp", "unit/test_d2q9_collision.cpp", "unit/test_d3q19_moments.cpp",
+    "unit/test_d3q19_collision.cpp", "unit/test_forces_momentum_exchange.cpp",
+    "validation/test_poiseuille_convergence.cpp", "validation/test_taylor_green_decay.cpp",
+]
+
+
+def build_reference_tests(lib_dir: Path, verbose: bool = False) -> list[Path]:
+    """Compile the reference's hot-path tests from their sources against libwake_b200.so.
+
+    The host sources (LatticeGrid2D/3D, memory, Strouhal) are the reference's, compiled
+    unchanged; only the kernel library differs. Asserts stay enabled (no -DNDEBUG).
+    Outputs go to oracle/_ref/reftests and find the GPU library via an $ORIGIN rpath.
+    """
+    ref = reference_dir()
+    out_dir = OUT / "reftests"
+    out_dir.mkdir(parents=True, exist_ok=True)
+    host = [ref / "src" / "grid" / "lattice_grid_2d.cpp", ref / "src" / "grid" / "lattice_grid_3d.cpp",
+            ref / "src" / "core" / "memory.cpp", ref / "src" / "forces" / "strouhal_analyzer.cpp",
+            ref / "src" / "forces" / "aerodynamic_telemetry.cpp"]
+    rel = os.path.relpath(lib_dir, out_dir)
+    built = []
+    for t in REFERENCE_TESTS:
+        exe = out_dir / Path(t).stem
+        cmd = ["g++", "-std=c++20", "-O2", f"-I{ref / 'include'}", str(ref / "tests" / t), *map(str, host),
+               f"-L{lib_dir}", "-lwake_b200", f"-Wl,-rpath,$ORIGIN/{rel}", "-o", str(exe)]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        built.append(exe)
+    return built
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv))
+    if "--tests" in sys.argv:
+        print(build_reference_tests(HERE.parent / "wake_b200", verbose="-v" in sys.argv))

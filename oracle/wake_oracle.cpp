@@ -68,8 +68,9 @@ struct D3Q27T {
     static constexpr int cx[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1};
     static constexpr int cy[27] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, 1, -1, -1, 1, 1, -1, -1};
     static constexpr int cz[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1, 1, 1, 1, 1, -1, -1, -1, -1};
+    // true opposites; the reference's table (lbm_d3q27.isph:35-40) mis-pairs the corners
     static constexpr int opp[27] = {0, 2, 1, 4, 3, 6, 5, 10, 9, 8, 7, 14, 13, 12, 11, 18, 17, 16, 15,
-                                    22, 21, 20, 19, 26, 25, 24, 23};
+                                    26, 25, 24, 23, 22, 21, 20, 19};
     static constexpr double wn[27] = {64, 16, 16, 16, 16, 16, 16, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4,
                                       1, 1, 1, 1, 1, 1, 1, 1};  // w = wn / 216
     static constexpr double wd = 216.0;

@@ -112,9 +112,9 @@ def tgv_case(R):
     R.ref3d_set_periodic(g._h, 1)
     g.init_fields(c.rho, c.ux, c.uy, c.uz)
     f0 = g.f()
-    g.step(60, 2)
+    g.step(30, 2)
     m = g.macro()
-    save("tgv3d_mrt", f0=f0, steps=np.int32(60), tau=np.float32(c.tau), rho=m["rho"], ux=m["ux"], uy=m["uy"],
+    save("tgv3d_mrt", f0=f0, steps=np.int32(30), tau=np.float32(c.tau), rho=m["rho"], ux=m["ux"], uy=m["uy"],
          uz=m["uz"])
 
 

@@ -154,7 +154,15 @@ struct wake_grid {
 
     DevMem A, B;       // state buffers
     int cur = 0;       // 0: A holds the current state, 1: B
-    bool direct = true;  // the non-current buffer holds f^k itself (right after initialisation)
+    // State machine. m_f (FP32) holds the reference-visible f^k whenever mf_valid.
+    // `pending`: A/B do not hold Collide(f^k) for the current collision parameters
+    // (fresh initial state, or tau / model / body force changed since the last
+    // collide); the next step re-collides f^k from m_f first, exactly like the
+    // reference, whose step k+1 starts by colliding f^k with that step's parameters.
+    bool pending = true;
+    bool mf_valid = false;
+    float collided_g[3] = {0.f, 0.f, 0.f};  // body force the state buffers were collided with
+    float last_step_g[3] = {0.f, 0.f, 0.f};  // body force of the last executed step
     DevMem d_types, d_flags, d_status, d_nodestart;
     std::vector<uint8_t> types;
     bool geom_dirty = true;
@@ -371,39 +379,73 @@ int ensure_macro(wake_grid* g) {
     return WAKE_OK;
 }
 
-// Write the reference-visible f^k (and/or macroscopic fields) into the scratch buffers.
+// Physics for reporting the state after the last step: the moments carry the
+// Guo shift of the body force that step used (lattice_grid_2d.cpp:257-259);
+// before any step there is none (initialize() stores the fields as given).
+Physics report_phys(const wake_grid* g) {
+    Physics p = g->phys;
+    for (int a = 0; a < 3; ++a) p.g[a] = g->k > 0 ? g->last_step_g[a] : 0.f;
+    return p;
+}
+
+// Bring the reference-visible f^k (into m_f) and/or its moments (into the
+// macro scratch) up to date. Uses the current device flags, i.e. the geometry
+// the last step ran with, as the reference's f_src is untouched by setters.
 int materialise(wake_grid* g, bool want_f, bool want_macro) {
-    if (want_f) WK_CUDA(g->m_f.ensure(sizeof(float) * g->Q * g->pitch));
     if (want_macro) {
         const int r = ensure_macro(g);
         if (r) return r;
     }
+    const Physics rp = report_phys(g);
+    if (g->mf_valid) {
+        if (!want_macro) return WAKE_OK;
+        const Out o = scratch_out(g, false, true);
+        WK_CUDA(launch_materialise_any(g->Q, STORE_F32, g->m_f.p, g->d_flags.as<uint8_t>(), g->geo(), g->links(), rp, o,
+                                       g->launch(), 1));
+        return WAKE_OK;
+    }
+    if (want_f) WK_CUDA(g->m_f.ensure(sizeof(float) * g->Q * g->pitch));
     const Out o = scratch_out(g, want_f, want_macro);
-    const void* src = g->buf(1 - g->cur);
-    WK_CUDA(launch_materialise_any(g->Q, g->storage, src, g->d_flags.as<uint8_t>(), g->geo(), g->links(), g->phys, o,
-                                   g->launch(), g->direct ? 1 : 0));
+    WK_CUDA(launch_materialise_any(g->Q, g->storage, g->buf(1 - g->cur), g->d_flags.as<uint8_t>(), g->geo(),
+                                   g->links(), rp, o, g->launch(), 0));
+    if (want_f) g->mf_valid = true;
     return WAKE_OK;
 }
 
-// Initial collide from the FP32 populations in m_f (flags must be current).
+// Collide f^k (FP32 in m_f) with the current parameters: A <- Collide(f^k), B <- f^k.
 int initial_from_scratch(wake_grid* g) {
     WK_CUDA(launch_initial_any(g->Q, g->collision, g->storage, g->les != 0, g->m_f.as<float>(), g->A.p, g->B.p,
                                g->d_flags.as<uint8_t>(), g->geo(), g->phys, g->launch()));
     g->cur = 0;
-    g->direct = true;
+    g->pending = false;
+    for (int a = 0; a < 3; ++a) g->collided_g[a] = g->phys.g[a];
     g->invalidate_graph();
     return WAKE_OK;
 }
 
-// Bring flags in line with the host geometry. If the cell types changed, the
-// reference-visible state f^k is re-derived with the old flags and the
-// collided buffer rebuilt with the new ones (the reference keeps f_src as is).
-int prepare(wake_grid* g) {
+// Called at the start of a step (phys holds that step's parameters). If the
+// geometry or any collision parameter changed, f^k is re-derived with the old
+// flags, the flags rebuilt and f^k re-collided with the new parameters.
+int apply_geometry(wake_grid* g) {
     if (!g->geom_dirty) return WAKE_OK;
-    int r = materialise(g, true, false);
+    if (!g->mf_valid) {
+        const int r = materialise(g, true, false);  // f^k under the old flags
+        if (r) return r;
+    }
+    const int r = rebuild_flags(g);
     if (r) return r;
-    r = rebuild_flags(g);
+    g->pending = true;
+    return WAKE_OK;
+}
+
+int prepare(wake_grid* g) {
+    const int r = apply_geometry(g);
     if (r) return r;
+    if (!g->pending) return WAKE_OK;
+    if (!g->mf_valid) {
+        const int r2 = materialise(g, true, false);
+        if (r2) return r2;
+    }
     return initial_from_scratch(g);
 }
 
@@ -411,14 +453,11 @@ int upload_f0(wake_grid* g, const float* f, cudaMemcpyKind kind) {
     WK_CUDA(g->m_f.ensure(sizeof(float) * g->Q * g->pitch));
     WK_CUDA(cudaMemcpy2DAsync(g->m_f.p, sizeof(float) * g->pitch, f, sizeof(float) * g->N, sizeof(float) * g->N,
                               g->Q, kind, g->stream));
-    if (g->geom_dirty) {
-        const int r = rebuild_flags(g);
-        if (r) return r;
-    }
-    const int r = initial_from_scratch(g);
-    if (r) return r;
-    g->k = 0;
     WK_CUDA(cudaStreamSynchronize(g->stream));
+    g->mf_valid = true;
+    g->pending = true;
+    g->k = 0;
+    g->invalidate_graph();
     return WAKE_OK;
 }
 
@@ -459,7 +498,8 @@ int do_steps(wake_grid* g, int n) {
         a.xchunks = g->xchunks;
         WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, a, g->launch()));
         g->cur ^= 1;
-        g->direct = false;
+        g->mf_valid = false;
+        for (int c = 0; c < 3; ++c) g->last_step_g[c] = g->phys.g[c];
         ++g->k;
     }
     return WAKE_OK;
@@ -561,6 +601,7 @@ int wake_grid_set_model(wake_grid* g, int collision, int les, float cs_smag, flo
     g->phys.mrt_exact = mrt_exact ? 1 : 0;
     g->phys.s3 = s3;
     g->phys.s4 = s4;
+    g->pending = true;  // the next step collides f^k with the new model
     g->invalidate_graph();
     return WAKE_OK;
 }
@@ -569,6 +610,7 @@ int wake_grid_set_relaxation_time(wake_grid* g, float tau) {
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
     if (!(tau > 0.5f)) return set_error(WAKE_ERR_INVALID, "tau must exceed 1/2");
     g->phys.tau = tau;
+    g->pending = true;
     g->invalidate_graph();
     return WAKE_OK;
 }
@@ -859,11 +901,14 @@ int wake_grid_get_force_history(wake_grid* g, double* out, int max) {
 int wake_grid_step(wake_grid* g, int n, float gx, float gy, float gz) {
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
     if (n < 0) return set_error(WAKE_ERR_INVALID, "negative step count");
+    if (n == 0) return WAKE_OK;
+    const float gnew[3] = {gx, gy, (g->D == 3) ? gz : 0.f};
+    for (int a = 0; a < 3; ++a) g->phys.g[a] = gnew[a];
+    // the buffers hold Collide(f^k) for the body force they were collided with;
+    // the reference collides f^k with this step's force, so re-collide on a change
+    if (gnew[0] != g->collided_g[0] || gnew[1] != g->collided_g[1] || gnew[2] != g->collided_g[2]) g->pending = true;
     int r = prepare(g);
     if (r) return r;
-    const float gnew[3] = {gx, gy, (g->D == 3) ? gz : 0.f};
-    if (gnew[0] != g->phys.g[0] || gnew[1] != g->phys.g[1] || gnew[2] != g->phys.g[2]) g->invalidate_graph();
-    for (int a = 0; a < 3; ++a) g->phys.g[a] = gnew[a];
     int done = 0;
     if (g->graph_steps > 0 && n >= g->graph_steps) {
         // (re)capture a graph of graph_steps launches from the current parity
@@ -892,7 +937,8 @@ int wake_grid_step(wake_grid* g, int n, float gx, float gy, float gz) {
         while (n - done >= gs && g->cur == g->graph_cur) {
             WK_CUDA(cudaGraphLaunch(g->graph, g->stream));
             g->k += gs;
-            g->direct = false;
+            g->mf_valid = false;
+            for (int c = 0; c < 3; ++c) g->last_step_g[c] = g->phys.g[c];
             done += gs;
         }
     }
@@ -921,9 +967,7 @@ int wake_grid_synchronize(wake_grid* g) {
 
 int wake_grid_get_populations(wake_grid* g, float* f) {
     if (!valid_grid(g) || !f) return set_error(WAKE_ERR_INVALID, "null output");
-    int r = prepare(g);
-    if (r) return r;
-    r = materialise(g, true, false);
+    const int r = materialise(g, true, false);
     if (r) return r;
     WK_CUDA(cudaMemcpy2DAsync(f, sizeof(float) * g->N, g->m_f.p, sizeof(float) * g->pitch, sizeof(float) * g->N, g->Q,
                               cudaMemcpyDefault, g->stream));
@@ -933,9 +977,7 @@ int wake_grid_get_populations(wake_grid* g, float* f) {
 
 int wake_grid_get_macroscopic(wake_grid* g, float* rho, float* ux, float* uy, float* uz, float* speed) {
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
-    int r = prepare(g);
-    if (r) return r;
-    r = materialise(g, false, true);
+    const int r = materialise(g, false, true);
     if (r) return r;
     const std::size_t b = sizeof(float) * g->N;
     if (rho) WK_CUDA(cudaMemcpyAsync(rho, g->m_rho.p, b, cudaMemcpyDefault, g->stream));
@@ -948,7 +990,7 @@ int wake_grid_get_macroscopic(wake_grid* g, float* rho, float* ux, float* uy, fl
 }
 
 static int diag_all(wake_grid* g, double out[4]) {
-    int r = prepare(g);
+    int r = apply_geometry(g);  // the sums run over the current cell types
     if (r) return r;
     r = materialise(g, false, true);
     if (r) return r;

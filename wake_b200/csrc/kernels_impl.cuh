@@ -106,8 +106,7 @@ __global__ void __launch_bounds__(512) k_direct(const void* fin_v, const uint8_t
     }
     if (out.rho) {
         float rho, u[3];
-        const float g0[3] = {0.f, 0.f, 0.f};
-        node_moments<Q>(f, g0, rho, u);
+        node_moments<Q>(f, phys.g, rho, u);
         out.rho[i] = rho;
         out.ux[i] = u[0];
         out.uy[i] = u[1];
@@ -115,7 +114,6 @@ __global__ void __launch_bounds__(512) k_direct(const void* fin_v, const uint8_t
         out.speed[i] = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
     }
     (void)flags;
-    (void)phys;
 }
 
 namespace {

@@ -104,8 +104,10 @@ struct Lat<27> {
         return t[q];
     }
     __host__ __device__ static constexpr int opp(int q) {
+        // true opposites (c_opp = -c). The reference's table (lbm_d3q27.isph:35-40) pairs the
+        // corners 19..26 with their x/y mirror images instead; see ref_opp_d3q27.
         constexpr int t[27] = {0, 2, 1, 4, 3, 6, 5, 10, 9, 8, 7, 14, 13, 12, 11, 18, 17, 16, 15,
-                               22, 21, 20, 19, 26, 25, 24, 23};
+                               26, 25, 24, 23, 22, 21, 20, 19};
         return t[q];
     }
     __host__ __device__ static constexpr float w(int q) {
@@ -263,6 +265,43 @@ __device__ __forceinline__ void collide_trt(float* f, float rho, const float u[3
         const float da = oa * (fa - odd) - Fa;
         f[q] = f[q] - ds - da;
         f[o] = f[o] - ds + da;
+    }
+}
+
+// The reference's D3Q27 "opposite" table (include/wake/ispc/lbm_d3q27.isph:35-40):
+// equal to the true opposite except that corner q pairs with its (x, y) mirror.
+__host__ __device__ constexpr int ref_opp_d3q27(int q) {
+    constexpr int t[27] = {0, 2, 1, 4, 3, 6, 5, 10, 9, 8, 7, 14, 13, 12, 11, 18, 17, 16, 15,
+                           22, 21, 20, 19, 26, 25, 24, 23};
+    return t[q];
+}
+
+// TRT exactly as d3q27_collision_mrt.ispc:60-88 computes it, with the
+// reference's pairing table: symmetric / antisymmetric parts of f and feq taken
+// against ref_opp_d3q27(q). Used only by the drop-in d3q27_collide entry point.
+__device__ __forceinline__ void collide_trt_d3q27_reference(float* f, float rho, const float u[3], const float g[3],
+                                                            float tau_s, float tau_a) {
+    using L = Lat<27>;
+    const float os = 1.0f / tau_s, oa = 1.0f / tau_a;
+    const float ps = 1.0f - 0.5f * os, pa = 1.0f - 0.5f * oa;
+    const float u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const float ug = u[0] * g[0] + u[1] * g[1] + u[2] * g[2];
+    float fe[27], in[27];
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        fe[q] = feq<27>(q, rho, u[0], u[1], u[2], u2);
+        in[q] = f[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const int o = ref_opp_d3q27(q);
+        const float fs = 0.5f * (in[q] + in[o]), fa = 0.5f * (in[q] - in[o]);
+        const float es = 0.5f * (fe[q] + fe[o]), ea = 0.5f * (fe[q] - fe[o]);
+        const float cu = float(L::cx(q)) * u[0] + float(L::cy(q)) * u[1] + float(L::cz(q)) * u[2];
+        const float cg = float(L::cx(q)) * g[0] + float(L::cy(q)) * g[1] + float(L::cz(q)) * g[2];
+        const float Fa = pa * L::w(q) * rho * (3.0f * cg);
+        const float Fs = ps * L::w(q) * rho * (-3.0f * ug + 9.0f * cu * cg);
+        f[q] = in[q] - os * (fs - es) - oa * (fa - ea) + Fs + Fa;
     }
 }
 

@@ -39,8 +39,10 @@ class Stager {
     T* in(const T* p, std::size_t n) { return static_cast<T*>(add(const_cast<T*>(p), n * sizeof(T), true, false)); }
     template <class T>
     T* inout(T* p, std::size_t n) { return static_cast<T*>(add(p, n * sizeof(T), true, true)); }
+    // Outputs are copied in as well: like the reference, kernels leave some
+    // entries (e.g. moments at solid nodes) untouched, and those keep the caller's values.
     template <class T>
-    T* out(T* p, std::size_t n) { return static_cast<T*>(add(p, n * sizeof(T), false, true)); }
+    T* out(T* p, std::size_t n) { return static_cast<T*>(add(p, n * sizeof(T), true, true)); }
 
     // Allocate the arena and copy staged inputs. Returns 0 or an error code.
     int begin() {
@@ -56,7 +58,6 @@ class Stager {
         }
         return WAKE_OK;
     }
-    void* dev(int k) const { return items_[k].dev; }
     // Copy staged outputs back and wait for the device.
     int end() {
         WK_CUDA(cudaGetLastError());
@@ -120,6 +121,7 @@ __global__ void k_collide(const float* __restrict__ fin, float* __restrict__ fou
     uy[i] = u[1];
     if (uz) uz[i] = u[2];
     if (COLL == COLL_BGK) collide_bgk<Q>(f, r, u, g, p0);
+    else if (COLL == COLL_TRT && Q == 27) collide_trt_d3q27_reference(f, r, u, g, p0, p1);
     else if (COLL == COLL_TRT) collide_trt<Q>(f, r, u, g, p0, p1);
     else if constexpr (Q == 9) collide_mrt_d2q9(f, r, u, g, p0, p1);
     else collide_mrt_d3q19(f, r, u, g, p0, p1, 0);
@@ -333,6 +335,8 @@ __global__ void k_bfl(float* fdst, const float* fsrc, const int* idx, const int*
     if (k >= nl) return;
     const long long n = static_cast<long long>(nx) * ny * nz;
     const int i = idx[k], q = qd[k];
+    // the links may come straight from device memory: skip malformed ones instead of faulting
+    if (i < 0 || i >= n || q < 1 || q >= 19) return;
     int cx, cy, cz, o;
     float w;
     rt_dir<19>(q, cx, cy, cz, o, w);

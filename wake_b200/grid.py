@@ -154,6 +154,8 @@ class _Grid:
             del out["uz"]
         return out
 
+    macro = macroscopic
+
     def rho_data(self) -> np.ndarray:
         return self.macroscopic()["rho"]
 
