@@ -114,6 +114,23 @@ void d3q19_compute_momentum_exchange_forces(const float f_post_collision[], cons
                                             int ny, int nz, float center_x, float center_y, float center_z,
                                             float max_radius, float* fx_out, float* fy_out, float* fz_out);
 
+/* Allocation-free variant of d3q19_compute_momentum_exchange_forces. It has no
+ * counterpart in the reference. It is meant for callers that cannot allocate
+ * device memory while they run: a serving loop that has committed all of HBM to
+ * resident lattices, or a latency-critical loop in which cudaMalloc / cudaFree
+ * would synchronise the device. Instead of allocating scratch, it keeps its
+ * per-block partial sums in a fixed 384 KiB device array of the library (held by
+ * every GPU that loads the library until the process exits), which limits the
+ * lattice to nx*ny*nz <= 4,194,304 nodes; larger sizes are rejected with
+ * WAKE_ERR_INVALID. Every pointer must be device or managed memory (host
+ * buffers would need allocated staging). Returns 0 or a WAKE_ERR_* code, and
+ * returns after the result is written. The first call on each device looks up
+ * the array's device address (once per device); make that first call before any
+ * stream capture. All calls share the array: calls that overlap on the GPU race. */
+int d3q19_compute_momentum_exchange_forces_noalloc(const float f_post_collision[], const uint8_t cell_type[], int nx,
+                                                   int ny, int nz, float center_x, float center_y, float center_z,
+                                                   float max_radius, float* fx_out, float* fy_out, float* fz_out);
+
 /* D3Q27: src/ispc/d3q27_collision_mrt.ispc:5-18 (TRT), d3q27_moments.ispc:4-11, d3q27_streaming.ispc:4-10 */
 void d3q27_collide(const float f_in[], float f_out[], const uint8_t cell_type[], float rho[], float ux[],
                    float uy[], float uz[], float tau_s, float tau_a, float gx, float gy, float gz, int count);

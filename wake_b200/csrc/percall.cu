@@ -8,6 +8,7 @@
 // which orders it after work the caller queued on that stream.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -683,6 +684,83 @@ void d3q19_compute_momentum_exchange_forces(const float f_post_collision[], cons
     mem_call<19>(f_post_collision, cell_type, nx, ny, nz, center_x, center_y, center_z, max_radius, fx_out, fy_out,
                  fz_out);
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- allocation-free momentum exchange
+// Some callers cannot allocate device memory while they run: a serving loop that
+// has committed all of HBM to resident lattices (an allocation would fail or
+// force an eviction), or a latency-critical loop in which cudaMalloc / cudaFree
+// would synchronise the device and stall the other streams. For them this
+// variant of d3q19_compute_momentum_exchange_forces keeps its scratch (one
+// FP64 partial sum per 256-node block) in a fixed array of this file instead of
+// allocating it. The array is 16384 blocks x 3 doubles = 384 KiB, so lattices of
+// up to 16384 x 256 = 4,194,304 nodes are accepted; every GPU that loads the
+// library keeps the array until the process exits.
+namespace {
+constexpr int kNoAllocMaxBlocks = 16384;
+constexpr long long kNoAllocMaxNodes = static_cast<long long>(kNoAllocMaxBlocks) * 256;
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_scratch_addr[kNoAllocMaxDevices] = {};
+}  // namespace
+
+static __device__ __align__(256) double g_noalloc_mem_partials[3 * kNoAllocMaxBlocks];
+
+static bool device_accessible(const void* p) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+extern "C" int d3q19_compute_momentum_exchange_forces_noalloc(const float f_post_collision[],
+                                                               const uint8_t cell_type[], int nx, int ny, int nz,
+                                                               float center_x, float center_y, float center_z,
+                                                               float max_radius, float* fx_out, float* fy_out,
+                                                               float* fz_out) {
+    if (nx <= 0 || ny <= 0 || nz <= 0)
+        return set_error(WAKE_ERR_INVALID, "momentum exchange (no-alloc): lattice sizes must be positive");
+    const long long n = static_cast<long long>(nx) * ny * nz;
+    if (n > kNoAllocMaxNodes)
+        return set_error(WAKE_ERR_INVALID, "momentum exchange (no-alloc): " + std::to_string(n) +
+                                               " nodes exceed the fixed scratch limit of " +
+                                               std::to_string(kNoAllocMaxNodes) + " nodes");
+    const void* ptrs[5] = {f_post_collision, cell_type, fx_out, fy_out, fz_out};
+    for (const void* p : ptrs)
+        if (!p || !device_accessible(p))
+            return set_error(WAKE_ERR_INVALID, "momentum exchange (no-alloc): every pointer must be device or "
+                                               "managed memory (host buffers would need allocated staging)");
+    int dev = 0;
+    WK_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return set_error(WAKE_ERR_INVALID, "momentum exchange (no-alloc): device ordinal out of range");
+    double* part = nullptr;
+    {
+        // one-time set-up per device, with that device current: the array's device address
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_scratch_addr[dev]) {
+            void* addr = nullptr;
+            WK_CUDA(cudaGetSymbolAddress(&addr, g_noalloc_mem_partials));
+            g_noalloc_scratch_addr[dev] = addr;
+        }
+        part = static_cast<double*>(g_noalloc_scratch_addr[dev]);
+    }
+    // one block per 256 nodes, so each block writes its own partial before the
+    // final kernel reads it: nothing from an earlier call is read back
+    const int nb = static_cast<int>((n + 255) / 256);
+    k_mem_partials<19><<<nb, 256>>>(f_post_collision, cell_type, nx, ny, nz, center_x, center_y, center_z, max_radius,
+                                     part);
+    WK_CUDA(cudaGetLastError());
+    k_mem_final<<<1, 32>>>(part, nb, fx_out, fy_out, fz_out);
+    WK_CUDA(cudaGetLastError());
+    WK_CUDA(cudaStreamSynchronize(0));
+    return WAKE_OK;
+}
+
+extern "C" {
 
 void d3q19_apply_curved_bfl(float f_dst[], const float f_src[], const int fluid_indices[], const int q_dirs[],
                             const float delta_fractions[], const float uw_x[], const float uw_y[], const float uw_z[],
