@@ -47,7 +47,23 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--graph", type=int, default=20, help="steps per captured CUDA graph (0: plain launches)")
+    p.add_argument("--profile", choices=["f32", "f16", "bf16"], default=None,
+                   help="profiling mode: only warm-up + timed steps of this storage, plain launches, one JSON line")
     return p.parse_args()
+
+
+def run_profile(args):
+    """Small command for ncu: the workload's fused step, nothing else."""
+    import torch
+
+    from wake_b200 import workloads as W
+
+    case = W.sphere_channel()
+    g = W.build_grid(case, storage=args.profile)
+    ms = timed_steps(g, case, args.steps, args.warmup, 1)
+    print(json.dumps({"profile": args.profile, "steps": args.steps, "ms_per_step": ms / args.steps,
+                      "mlups": case.n * args.steps / (ms * 1e-3) / 1e6}))
+    torch.cuda.synchronize()
 
 
 def hbm_peak():
@@ -251,6 +267,9 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference_impl(args)
+        return
+    if args.profile:
+        run_profile(args)
         return
     world, rank, local = dist_setup(args)
     import torch
