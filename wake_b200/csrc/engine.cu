@@ -57,10 +57,10 @@ struct HostLat {
     }
 };
 
-cudaError_t launch_step_any(int Q, int coll, int store, bool les, const StepArgs& a, const Launch& L) {
-    if (Q == 9) return launch_step_q9(coll, store, les, a, L);
-    if (Q == 19) return launch_step_q19(coll, store, les, a, L);
-    return launch_step_q27(coll, store, les, a, L);
+cudaError_t launch_step_any(int Q, int coll, int store, bool les, const StepArgs& a, const Launch& L, bool fast) {
+    if (Q == 9) return launch_step_q9(coll, store, les, a, L, fast);
+    if (Q == 19) return launch_step_q19(coll, store, les, a, L, fast);
+    return launch_step_q27(coll, store, les, a, L, fast);
 }
 cudaError_t launch_initial_any(int Q, int coll, int store, bool les, const float* f0, void* a, void* b,
                                const uint8_t* flags, const Geo& geo, const Physics& phys, const Launch& L) {
@@ -81,10 +81,10 @@ cudaError_t launch_flags_any(int Q, const uint8_t* types, uint8_t* flags, const 
     if (Q == 19) return launch_flags_q19(types, flags, geo, cfg, L);
     return launch_flags_q27(types, flags, geo, cfg, L);
 }
-cudaError_t launch_block_marks_any(int Q, const uint8_t* flags, int* marks, const Geo& geo, const Launch& L) {
-    if (Q == 9) return launch_block_marks_q9(flags, marks, geo, L);
-    if (Q == 19) return launch_block_marks_q19(flags, marks, geo, L);
-    return launch_block_marks_q27(flags, marks, geo, L);
+cudaError_t launch_row_class_any(int Q, const uint8_t* flags, uint8_t* cls, const Geo& geo, const Launch& L) {
+    if (Q == 9) return launch_row_class_q9(flags, cls, geo, L);
+    if (Q == 19) return launch_row_class_q19(flags, cls, geo, L);
+    return launch_row_class_q27(flags, cls, geo, L);
 }
 
 // ---------------------------------------------------------------- small kernels
@@ -182,7 +182,12 @@ struct wake_grid {
     float center[3] = {0.f, 0.f, 0.f}, rmax = 0.f;
     DevMem d_block_slot, d_partial, d_counters, d_hist;
 
-    int tpb = 0, xchunks = 1, rows = 1;
+    // rows handled by k_step_fast (pure-gather rows) and by k_step (the rest),
+    // packed (z << 16) | y; the k_step block of list entry b owns momentum slot block_slot[b]
+    DevMem d_fast_rows, d_gen_rows;
+    int n_fast = 0, n_gen = 0;
+
+    int tpb = 0, xchunks = 1, rows = 1, tpb_fast = 256;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     long long k = 0;
@@ -230,7 +235,7 @@ struct wake_grid {
         l.count = dev_links;
         return l;
     }
-    Launch launch() const { return Launch{tpb, xchunks, rows, stream}; }
+    Launch launch() const { return Launch{tpb, xchunks, rows, stream, ny, nz, tpb_fast}; }
     int blocks() const { return rows * xchunks; }
 
     void invalidate_graph() { graph_ok = false; }
@@ -254,6 +259,17 @@ struct wake_grid {
         }
         xchunks = (nx + tpb - 1) / tpb;
         rows = ny * nz;
+        // k_step_fast is limited to 256 threads (four blocks per SM): least idle lanes over the row
+        const int cap = std::min(want > 0 ? want : 256, 256);
+        int best = -1, best_waste = 1 << 30;
+        for (int t = cap; t >= 64; t -= 32) {
+            const int waste = ((nx + t - 1) / t) * t - nx;
+            if (waste < best_waste) {
+                best = t;
+                best_waste = waste;
+            }
+        }
+        tpb_fast = best > 0 ? best : 64;
     }
 };
 
@@ -298,22 +314,48 @@ int rebuild_flags(wake_grid* g) {
         WK_CUDA(launch_link_marks(g->d_link_node.as<int>(), nl, g->d_flags.as<uint8_t>(), g->d_nodestart.as<int>(),
                                   g->stream));
     }
-    if (g->mem_on) {
-        const int nb = g->blocks();
-        DevMem marks;
-        WK_CUDA(marks.ensure(sizeof(int) * nb));
-        WK_CUDA(launch_block_marks_any(g->Q, g->d_flags.as<uint8_t>(), marks.as<int>(), geo, g->launch()));
-        std::vector<int> h(nb);
-        WK_CUDA(cudaMemcpyAsync(h.data(), marks.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, g->stream));
+    // split the rows between the two step kernels
+    {
+        const int nr = g->rows;
+        DevMem cls;
+        WK_CUDA(cls.ensure(nr));
+        WK_CUDA(launch_row_class_any(g->Q, g->d_flags.as<uint8_t>(), cls.as<uint8_t>(), geo, g->launch()));
+        std::vector<uint8_t> h(nr);
+        WK_CUDA(cudaMemcpyAsync(h.data(), cls.p, nr, cudaMemcpyDeviceToHost, g->stream));
         WK_CUDA(cudaStreamSynchronize(g->stream));
+        std::vector<unsigned> fast, gen;
+        std::vector<int> slots;
         int slot = 0;
-        for (int b = 0; b < nb; ++b) h[b] = h[b] ? slot++ : -1;
-        if (slot == 0) h[0] = slot++;  // no link in range: block 0 still records a zero force every step
+        for (int r = 0; r < nr; ++r) {
+            const unsigned packed = (static_cast<unsigned>(r / g->ny) << 16) | static_cast<unsigned>(r % g->ny);
+            if ((h[r] & 1) && !(g->mem_on && slot == 0 && r == nr - 1 && gen.empty())) {
+                fast.push_back(packed);
+            } else {
+                gen.push_back(packed);
+                slots.push_back(g->mem_on && (h[r] & 2) ? slot++ : -1);
+            }
+        }
+        if (g->mem_on && slot == 0) {
+            // no momentum-exchange link in range: one k_step block still records a zero force every step
+            slots[0] = slot++;
+        }
+        g->n_fast = static_cast<int>(fast.size());
+        g->n_gen = static_cast<int>(gen.size());
         g->n_slots = slot;
-        WK_CUDA(g->d_block_slot.ensure(sizeof(int) * nb));
-        WK_CUDA(cudaMemcpyAsync(g->d_block_slot.p, h.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, g->stream));
-        WK_CUDA(g->d_partial.ensure(sizeof(double) * 3 * std::max(1, slot)));
-        WK_CUDA(cudaStreamSynchronize(g->stream));  // h goes out of scope
+        WK_CUDA(g->d_fast_rows.ensure(sizeof(unsigned) * std::max<std::size_t>(1, fast.size())));
+        WK_CUDA(g->d_gen_rows.ensure(sizeof(unsigned) * std::max<std::size_t>(1, gen.size())));
+        WK_CUDA(g->d_block_slot.ensure(sizeof(int) * std::max<std::size_t>(1, slots.size())));
+        if (!fast.empty())
+            WK_CUDA(cudaMemcpyAsync(g->d_fast_rows.p, fast.data(), sizeof(unsigned) * fast.size(),
+                                    cudaMemcpyHostToDevice, g->stream));
+        if (!gen.empty()) {
+            WK_CUDA(cudaMemcpyAsync(g->d_gen_rows.p, gen.data(), sizeof(unsigned) * gen.size(), cudaMemcpyHostToDevice,
+                                    g->stream));
+            WK_CUDA(cudaMemcpyAsync(g->d_block_slot.p, slots.data(), sizeof(int) * slots.size(),
+                                    cudaMemcpyHostToDevice, g->stream));
+        }
+        if (g->mem_on) WK_CUDA(g->d_partial.ensure(sizeof(double) * 3 * std::max(1, slot)));
+        WK_CUDA(cudaStreamSynchronize(g->stream));  // the host vectors go out of scope
     }
     g->geom_dirty = false;
     g->invalidate_graph();
@@ -495,8 +537,13 @@ int do_steps(wake_grid* g, int n) {
             if (g->n_slots == 0) a.mem.enabled = 0;
         }
         a.phys = g->phys;
-        a.xchunks = g->xchunks;
-        WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, a, g->launch()));
+        // pure-gather rows first, then the rows with boundaries and momentum exchange
+        a.rows = g->d_fast_rows.as<unsigned>();
+        a.nrows = g->n_fast;
+        WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, a, g->launch(), true));
+        a.rows = g->d_gen_rows.as<unsigned>();
+        a.nrows = g->n_gen;
+        WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, a, g->launch(), false));
         g->cur ^= 1;
         g->mf_valid = false;
         for (int c = 0; c < 3; ++c) g->last_step_g[c] = g->phys.g[c];
@@ -522,8 +569,8 @@ wake_grid* wake_grid_create(int q, int nx, int ny, int nz, float tau, int storag
         return nullptr;
     }
     const long long N = static_cast<long long>(nx) * ny * nz;
-    if (N >= (1ll << 31)) {
-        set_error(WAKE_ERR_INVALID, "wake_grid_create: more than 2^31 - 1 nodes");
+    if (N >= (1ll << 31) || ny > 65535 || nz > 65535) {
+        set_error(WAKE_ERR_INVALID, "wake_grid_create: more than 2^31 - 1 nodes, or ny / nz above 65535");
         return nullptr;
     }
     auto* g = new wake_grid(q);

@@ -13,6 +13,8 @@ struct Launch {
     int xchunks;   // blocks per row
     int rows;      // ny * nz
     cudaStream_t stream;
+    int ny, nz;
+    int tpb_fast;  // threads per block of k_step_fast (<= 256)
 };
 
 struct FlagCfg {
@@ -25,7 +27,7 @@ struct FlagCfg {
 
 // Per-lattice entry points (defined once per Q in kernels_impl.cuh).
 #define WK_DECLARE_LAUNCHERS(Q)                                                                                   \
-    cudaError_t launch_step_q##Q(int coll, int store, bool les, const StepArgs& a, const Launch& L);             \
+    cudaError_t launch_step_q##Q(int coll, int store, bool les, const StepArgs& a, const Launch& L, bool fast);  \
     cudaError_t launch_materialise_q##Q(int store, const void* fin, const uint8_t* flags, const Geo& geo,        \
                                         const Links& links, const Physics& phys, const Out& out,                 \
                                         const Launch& L, int direct);                                            \
@@ -33,7 +35,7 @@ struct FlagCfg {
                                     const uint8_t* flags, const Geo& geo, const Physics& phys, const Launch& L); \
     cudaError_t launch_flags_q##Q(const uint8_t* types, uint8_t* flags, const Geo& geo, const FlagCfg& cfg,      \
                                   const Launch& L);                                                              \
-    cudaError_t launch_block_marks_q##Q(const uint8_t* flags, int* marks, const Geo& geo, const Launch& L);
+    cudaError_t launch_row_class_q##Q(const uint8_t* flags, uint8_t* cls, const Geo& geo, const Launch& L);
 
 WK_DECLARE_LAUNCHERS(9)
 WK_DECLARE_LAUNCHERS(19)

@@ -37,7 +37,8 @@ __global__ void k_flags(const uint8_t* __restrict__ types, uint8_t* __restrict__
             if (cfg.inflow && x == 0 && t == CT_INFLOW) { fl |= FL_ZH_IN; zh = true; }
             if (cfg.outflow && x == nx - 1 && t == CT_OUTFLOW) { fl |= FL_ZH_OUT; zh = true; }
         }
-        bool fast = !zh;
+        bool fast = true;  // Zou-He nodes gather purely too; the formula is applied after the gather
+        (void)zh;
         bool mem = false;
 #pragma unroll
         for (int q = 1; q < Q; ++q) {
@@ -75,15 +76,20 @@ __global__ void k_flags(const uint8_t* __restrict__ types, uint8_t* __restrict__
     flags[i] = fl;
 }
 
+// Row classes for the two step kernels: bit 0 = every node of the row is a pure
+// gather (k_step_fast), bit 1 = the row holds a momentum-exchange node.
 template <int Q>
-__global__ void k_block_marks(const uint8_t* __restrict__ flags, int* __restrict__ marks, const Geo geo,
-                              int xchunks) {
-    const int row = blockIdx.x / xchunks;
-    const int x = (blockIdx.x - row * xchunks) * blockDim.x + threadIdx.x;
-    bool mine = false;
-    if (x < geo.nx) mine = (flags[static_cast<long long>(row) * geo.nx + x] & FL_MEM) != 0;
-    const int any = __syncthreads_or(mine ? 1 : 0);
-    if (threadIdx.x == 0) marks[blockIdx.x] = any;
+__global__ void k_row_class(const uint8_t* __restrict__ flags, uint8_t* __restrict__ cls, const Geo geo) {
+    const long long row0 = static_cast<long long>(blockIdx.x) * geo.nx;
+    int all_fast = 1, any_mem = 0;
+    for (int x = threadIdx.x; x < geo.nx; x += blockDim.x) {
+        const uint8_t fl = flags[row0 + x];
+        all_fast &= (fl & FL_FAST) ? 1 : 0;
+        any_mem |= (fl & FL_MEM) ? 1 : 0;
+    }
+    all_fast = __syncthreads_and(all_fast);
+    any_mem = __syncthreads_or(any_mem);
+    if (threadIdx.x == 0) cls[blockIdx.x] = static_cast<uint8_t>((all_fast ? 1 : 0) | (any_mem ? 2 : 0));
 }
 
 // Pull-free read of f^0 (state buffer holding pre-collision populations).
@@ -120,15 +126,17 @@ namespace {
 constexpr int kQ = WK_Q;
 
 template <int C, int S, bool LES>
-void step_one(const StepArgs& a, const Launch& L) {
-    k_step<kQ, C, S, LES><<<L.rows * L.xchunks, L.tpb, 0, L.stream>>>(a);
+void step_one(const StepArgs& a, const Launch& L, bool fast) {
+    if (a.nrows <= 0) return;
+    if (fast) k_step_fast<kQ, C, S, LES><<<a.nrows, L.tpb_fast, 0, L.stream>>>(a);
+    else k_step<kQ, C, S, LES><<<a.nrows, L.tpb, 0, L.stream>>>(a);
 }
 template <int C, int S, bool LES>
 void initial_one(const float* f0, void* A, void* B, const uint8_t* flags, const Geo& g, const Physics& p,
                  const Launch& L) {
     k_initial<kQ, C, S, LES><<<L.rows * L.xchunks, L.tpb, 0, L.stream>>>(f0, A, B, flags, g, p, L.xchunks);
 }
-using StepFn = void (*)(const StepArgs&, const Launch&);
+using StepFn = void (*)(const StepArgs&, const Launch&, bool);
 using InitFn = void (*)(const float*, void*, void*, const uint8_t*, const Geo&, const Physics&, const Launch&);
 
 #define WK_ROW(C, S) {step_one<C, S, false>, step_one<C, S, true>}
@@ -145,9 +153,10 @@ const InitFn kInit[3][3][2] = {{WK_IROW(0, 0), WK_IROW(0, 1), WK_IROW(0, 2)},
 bool valid(int coll, int store) { return coll >= 0 && coll < 3 && store >= 0 && store < 3; }
 }  // namespace
 
-cudaError_t WK_CAT(launch_step_q, WK_Q)(int coll, int store, bool les, const StepArgs& a, const Launch& L) {
+cudaError_t WK_CAT(launch_step_q, WK_Q)(int coll, int store, bool les, const StepArgs& a, const Launch& L,
+                                       bool fast) {
     if (!valid(coll, store)) return cudaErrorInvalidValue;
-    kStep[coll][store][les ? 1 : 0](a, L);
+    kStep[coll][store][les ? 1 : 0](a, L, fast);
     return cudaGetLastError();
 }
 
@@ -187,8 +196,8 @@ cudaError_t WK_CAT(launch_flags_q, WK_Q)(const uint8_t* types, uint8_t* flags, c
     return cudaGetLastError();
 }
 
-cudaError_t WK_CAT(launch_block_marks_q, WK_Q)(const uint8_t* flags, int* marks, const Geo& geo, const Launch& L) {
-    k_block_marks<kQ><<<L.rows * L.xchunks, L.tpb, 0, L.stream>>>(flags, marks, geo, L.xchunks);
+cudaError_t WK_CAT(launch_row_class_q, WK_Q)(const uint8_t* flags, uint8_t* cls, const Geo& geo, const Launch& L) {
+    k_row_class<kQ><<<L.rows, 256, 0, L.stream>>>(flags, cls, geo);
     return cudaGetLastError();
 }
 

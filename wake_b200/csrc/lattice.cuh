@@ -130,6 +130,8 @@ struct Codec<STORE_F32> {
     __device__ static __forceinline__ float load(const T* p, float) { return __ldg(p); }
     __device__ static __forceinline__ float load_plain(const T* p, float) { return *p; }
     __device__ static __forceinline__ void store(T* p, float v, float) { *p = v; }
+    // evict-first store for the step output: it is read again only in the next step
+    __device__ static __forceinline__ void store_stream(T* p, float v, float) { __stcs(p, v); }
     __host__ __device__ static float decode(T v, float) { return v; }
 };
 
@@ -142,6 +144,9 @@ struct Codec<STORE_F16> {
     __device__ static __forceinline__ float load_plain(const T* p, float w) { return fmaf(w, __half2float(*p), w); }
     __device__ static __forceinline__ void store(T* p, float v, float w) {
         *p = __float2half_rn(fmaf(v, 1.0f / w, -1.0f));
+    }
+    __device__ static __forceinline__ void store_stream(T* p, float v, float w) {
+        __stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(__float2half_rn(fmaf(v, 1.0f / w, -1.0f))));
     }
 };
 
@@ -156,6 +161,10 @@ struct Codec<STORE_BF16> {
     }
     __device__ static __forceinline__ void store(T* p, float v, float w) {
         *p = __float2bfloat16_rn(fmaf(v, 1.0f / w, -1.0f));
+    }
+    __device__ static __forceinline__ void store_stream(T* p, float v, float w) {
+        __stcs(reinterpret_cast<unsigned short*>(p),
+               __bfloat16_as_ushort(__float2bfloat16_rn(fmaf(v, 1.0f / w, -1.0f))));
     }
 };
 
@@ -200,14 +209,21 @@ __device__ __forceinline__ void node_moments(const float* f, const float g[3], f
 
 // Smagorinsky tau from the local non-equilibrium stress (d2q9_les.ispc:19-55,
 // d3q19_les.ispc:21-64), applied per node.
+// Because c_opp = -c, the second-order tensor only sees the even part of each
+// (q, opp) pair: Pi = sum over pairs c c^T (f_q + f_opp - 2 w rho (1 + 4.5 (c.u)^2 - 1.5 u^2)).
+// The same even parts feed the TRT update, so the compiler shares them.
 template <int Q>
 __device__ __forceinline__ float smagorinsky_tau(const float* f, float rho, const float u[3], float tau0, float cs) {
     using L = Lat<Q>;
     const float u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
     float pxx = 0.f, pyy = 0.f, pzz = 0.f, pxy = 0.f, pyz = 0.f, pxz = 0.f;
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        const float fn = f[q] - feq<Q>(q, rho, u[0], u[1], u[2], u2);
+    for (int q = 1; q < Q; ++q) {
+        const int o = L::opp(q);
+        if (o < q) continue;
+        const float cu = float(L::cx(q)) * u[0] + float(L::cy(q)) * u[1] + float(L::cz(q)) * u[2];
+        const float base = L::w(q) * rho * (1.0f + 4.5f * cu * cu - 1.5f * u2);
+        const float fn = (f[q] + f[o]) - 2.0f * base;
         const int x = L::cx(q), y = L::cy(q), z = L::cz(q);
         if (x) pxx += fn;
         if (y) pyy += fn;

@@ -69,6 +69,35 @@ __device__ __forceinline__ int wrap(int v, int n) {
     return v;
 }
 
+// Pure gather of a node whose pull sources are all in range (after the periodic
+// wraps) and plain fluid: the three x positions and the row bases of the
+// (dy, dz) shifts are built once, then each load is a warp-uniform plane
+// pointer plus a 32-bit in-plane offset.
+template <int Q, int S>
+__device__ __forceinline__ void gather_pure(const typename Codec<S>::T* __restrict__ fin, const Geo& G, int x, int y,
+                                            int z, float f[Q]) {
+    using L = Lat<Q>;
+    using C = Codec<S>;
+    const long long P = G.pitch;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const int xs[3] = {x == nx - 1 ? 0 : x + 1, x, x == 0 ? nx - 1 : x - 1};  // source x for cx = -1, 0, +1
+    int ys[3] = {y + 1, y, y - 1}, zs[3] = {z + 1, z, z - 1};                // source rows for c = -1, 0, +1
+    if (G.periodic_y) {
+        ys[0] = ys[0] == ny ? 0 : ys[0];
+        ys[2] = ys[2] < 0 ? ny - 1 : ys[2];
+    }
+    if (G.periodic_z) {
+        zs[0] = zs[0] == nz ? 0 : zs[0];
+        zs[2] = zs[2] < 0 ? nz - 1 : zs[2];
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const unsigned off =
+            static_cast<unsigned>((zs[L::cz(q) + 1] * ny + ys[L::cy(q) + 1]) * nx + xs[L::cx(q) + 1]);
+        f[q] = C::load(fin + q * P + off, L::w(q));
+    }
+}
+
 // Pull f^{k+1}(x) out of g^k. `bb` gets bit q when the pull of q bounced off a
 // solid or moving-wall node (in range), which marks the momentum-exchange link
 // (x, opp(q)).
@@ -82,15 +111,9 @@ __device__ __forceinline__ void gather(const typename Codec<S>::T* __restrict__ 
     const int nx = G.nx, ny = G.ny, nz = G.nz;
     bb = 0u;
     if (fl & FL_FAST) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const int sx = L::cx(q) ? wrap<Q>(x - L::cx(q), nx) : x;
-            int sy = y - L::cy(q), sz = z - L::cz(q);
-            if (L::cy(q) && G.periodic_y) sy = wrap<Q>(sy, ny);
-            if (L::cz(q) && G.periodic_z) sz = wrap<Q>(sz, nz);
-            const long long s = (static_cast<long long>(sz) * ny + sy) * nx + sx;
-            f[q] = C::load(fin + q * P + s, L::w(q));
-        }
+        gather_pure<Q, S>(fin, G, x, y, z, f);
+        if (fl & FL_ZH_IN) zou_he_inlet<Q>(f, G.uin);
+        if (fl & FL_ZH_OUT) zou_he_outlet<Q>(f, G.rho_out);
         return;
     }
 #pragma unroll
@@ -231,7 +254,8 @@ struct StepArgs {
     Links links;
     MemCfg mem;
     Physics phys;
-    int xchunks;
+    const unsigned* rows;  // rows of this launch, packed (z << 16) | y; one block per row
+    int nrows;
 };
 
 // One fused time step: g^{k+1} = Collide(ZouHe(BFL(Pull(g^k)))). Solid nodes are not
@@ -241,31 +265,59 @@ __global__ void __launch_bounds__(512) k_step(const StepArgs a) {
     using L = Lat<Q>;
     using C = Codec<S>;
     using T = typename C::T;
-    const int row = blockIdx.x / a.xchunks;
-    const int x = (blockIdx.x - row * a.xchunks) * blockDim.x + threadIdx.x;
-    const int ny = a.geo.ny;
-    const int y = row % ny, z = row / ny;
+    // one block per listed row; the threads stride along x
+    const unsigned e = a.rows[blockIdx.x];
+    const int y = static_cast<int>(e & 0xffffu), z = static_cast<int>(e >> 16);
+    const long long row0 = (static_cast<long long>(z) * a.geo.ny + y) * a.geo.nx;
     double acc[3] = {0.0, 0.0, 0.0};
-    if (x < a.geo.nx) {
-        const long long i = static_cast<long long>(row) * a.geo.nx + x;
+    for (int x = threadIdx.x; x < a.geo.nx; x += blockDim.x) {
+        const long long i = row0 + x;
         const uint8_t fl = a.flags[i];
-        if ((fl & FL_TYPE) != CT_SOLID) {
-            float f[Q];
-            unsigned bb;
-            gather<Q, S>(static_cast<const T*>(a.fin), a.geo, a.flags, a.links, x, y, z, i, fl, f, bb);
-            float rho, u[3];
-            node_moments<Q>(f, a.phys.g, rho, u);
-            if (fl & FL_MEM) mem_node<Q>(f, bb, x, y, z, a.geo, a.mem, acc);
-            if (!(rho > 0.0f) || !(fabsf(u[0]) < 1e30f)) atomicOr(a.status, ERR_NONFINITE);
-            collide<Q, COLL, LES>(f, rho, u, a.phys);
-            T* out = static_cast<T*>(a.fout);
+        if ((fl & FL_TYPE) == CT_SOLID) continue;
+        float f[Q];
+        unsigned bb;
+        gather<Q, S>(static_cast<const T*>(a.fin), a.geo, a.flags, a.links, x, y, z, i, fl, f, bb);
+        float rho, u[3];
+        node_moments<Q>(f, a.phys.g, rho, u);
+        if (fl & FL_MEM) mem_node<Q>(f, bb, x, y, z, a.geo, a.mem, acc);
+        if (!(rho > 0.0f) || !(fabsf(u[0]) < 1e30f)) atomicOr(a.status, ERR_NONFINITE);
+        collide<Q, COLL, LES>(f, rho, u, a.phys);
+        T* out = static_cast<T*>(a.fout);
 #pragma unroll
-            for (int q = 0; q < Q; ++q) C::store(out + q * a.geo.pitch + i, f[q], L::w(q));
-        }
+        for (int q = 0; q < Q; ++q) C::store_stream(out + q * a.geo.pitch + i, f[q], L::w(q));
     }
     if (a.mem.enabled) {
         const int slot = a.mem.block_slot[blockIdx.x];
         if (slot >= 0) mem_block_finish(a.mem, acc, slot);
+    }
+}
+
+// The same step for rows whose every node is a pure gather (no solid, no
+// bounce-back, no curved link; Zou-He allowed) -- the bulk of a domain. Without
+// the rare paths the kernel fits 64 registers, i.e. four 256-thread blocks per SM.
+template <int Q, int COLL, int S, bool LES>
+__global__ void __launch_bounds__(256, 4) k_step_fast(const StepArgs a) {
+    using L = Lat<Q>;
+    using C = Codec<S>;
+    using T = typename C::T;
+    const unsigned e = a.rows[blockIdx.x];
+    const int y = static_cast<int>(e & 0xffffu), z = static_cast<int>(e >> 16);
+    const long long row0 = (static_cast<long long>(z) * a.geo.ny + y) * a.geo.nx;
+    const T* fin = static_cast<const T*>(a.fin);
+    T* out = static_cast<T*>(a.fout);
+    for (int x = threadIdx.x; x < a.geo.nx; x += blockDim.x) {
+        const long long i = row0 + x;
+        const uint8_t fl = a.flags[i];
+        float f[Q];
+        gather_pure<Q, S>(fin, a.geo, x, y, z, f);
+        if (fl & FL_ZH_IN) zou_he_inlet<Q>(f, a.geo.uin);
+        if (fl & FL_ZH_OUT) zou_he_outlet<Q>(f, a.geo.rho_out);
+        float rho, u[3];
+        node_moments<Q>(f, a.phys.g, rho, u);
+        if (!(rho > 0.0f) || !(fabsf(u[0]) < 1e30f)) atomicOr(a.status, ERR_NONFINITE);
+        collide<Q, COLL, LES>(f, rho, u, a.phys);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) C::store_stream(out + q * a.geo.pitch + i, f[q], L::w(q));
     }
 }
 
