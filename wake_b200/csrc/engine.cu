@@ -190,6 +190,8 @@ struct wake_grid {
     int tpb = 0, xchunks = 1, rows = 1, tpb_fast = 256;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t side = nullptr;  // forked stream of the general-row launch
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     long long k = 0;
 
     DevMem m_f, m_rho, m_ux, m_uy, m_uz, m_speed, m_diag;
@@ -204,6 +206,9 @@ struct wake_grid {
     ~wake_grid() {
         if (graph) cudaGraphExecDestroy(graph);
         if (own_stream && stream) cudaStreamDestroy(stream);
+        if (side) cudaStreamDestroy(side);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
     }
 
     void* buf(int which) { return which == 0 ? A.p : B.p; }
@@ -537,13 +542,27 @@ int do_steps(wake_grid* g, int n) {
             if (g->n_slots == 0) a.mem.enabled = 0;
         }
         a.phys = g->phys;
-        // pure-gather rows first, then the rows with boundaries and momentum exchange
+        // The pure-gather rows and the rows with boundaries / momentum exchange write
+        // disjoint nodes of the output, so the small general launch runs on a forked
+        // stream beside the bulk launch (a fork/join that CUDA graph capture keeps).
+        StepArgs gen = a;
+        gen.rows = g->d_gen_rows.as<unsigned>();
+        gen.nrows = g->n_gen;
         a.rows = g->d_fast_rows.as<unsigned>();
         a.nrows = g->n_fast;
+        const bool fork = g->n_fast > 0 && g->n_gen > 0;
+        Launch side = g->launch();
+        if (fork) {
+            side.stream = g->side;
+            WK_CUDA(cudaEventRecord(g->ev_fork, g->stream));
+            WK_CUDA(cudaStreamWaitEvent(g->side, g->ev_fork, 0));
+        }
+        WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, gen, side, false));
         WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, a, g->launch(), true));
-        a.rows = g->d_gen_rows.as<unsigned>();
-        a.nrows = g->n_gen;
-        WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, a, g->launch(), false));
+        if (fork) {
+            WK_CUDA(cudaEventRecord(g->ev_join, g->side));
+            WK_CUDA(cudaStreamWaitEvent(g->stream, g->ev_join, 0));
+        }
         g->cur ^= 1;
         g->mf_valid = false;
         for (int c = 0; c < 3; ++c) g->last_step_g[c] = g->phys.g[c];
@@ -594,6 +613,9 @@ wake_grid* wake_grid_create(int q, int nx, int ny, int nz, float tau, int storag
     g->choose_block(0);
     cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) g->own_stream = true;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming);
     const std::size_t sb = g->elem * static_cast<std::size_t>(q) * g->pitch;
     if (e == cudaSuccess) e = g->A.ensure(sb);
     if (e == cudaSuccess) e = g->B.ensure(sb);

@@ -254,34 +254,46 @@ __device__ __forceinline__ void collide_bgk(float* f, float rho, const float u[3
 }
 
 template <int Q>
-__device__ __forceinline__ void collide_trt(float* f, float rho, const float u[3], const float g[3], float tau_s,
-                                            float tau_a) {
+__device__ __forceinline__ void collide_trt_t(float* f, float rho, const float u[3], const float g[3], float tau_s,
+                                              float tau_a, bool forced) {
     using L = Lat<Q>;
     const float os = 1.0f / tau_s, oa = 1.0f / tau_a;
     const float ps = 1.0f - 0.5f * os, pa = 1.0f - 0.5f * oa;
     const float u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-    const float ug = u[0] * g[0] + u[1] * g[1] + u[2] * g[2];
+    const float ug = forced ? u[0] * g[0] + u[1] * g[1] + u[2] * g[2] : 0.0f;
     // rest population: symmetric only
     {
         const float fe = feq<Q>(0, rho, u[0], u[1], u[2], u2);
-        f[0] = f[0] - os * (f[0] - fe) + ps * L::w(0) * rho * (-3.0f * ug);
+        f[0] = f[0] - os * (f[0] - fe);
+        if (forced) f[0] += ps * L::w(0) * rho * (-3.0f * ug);
     }
 #pragma unroll
     for (int q = 1; q < Q; ++q) {
         const int o = L::opp(q);
         if (o < q) continue;  // handle each (q, opp) pair once
         const float cu = float(L::cx(q)) * u[0] + float(L::cy(q)) * u[1] + float(L::cz(q)) * u[2];
-        const float cg = float(L::cx(q)) * g[0] + float(L::cy(q)) * g[1] + float(L::cz(q)) * g[2];
         const float base = L::w(q) * rho * (1.0f + 4.5f * cu * cu - 1.5f * u2);  // even part of feq
         const float odd = L::w(q) * rho * 3.0f * cu;                             // odd part of feq
         const float fs = 0.5f * (f[q] + f[o]), fa = 0.5f * (f[q] - f[o]);
-        const float Fs = ps * L::w(q) * rho * (-3.0f * ug + 9.0f * cu * cg);
-        const float Fa = pa * L::w(q) * rho * (3.0f * cg);
-        const float ds = os * (fs - base) - Fs;
-        const float da = oa * (fa - odd) - Fa;
+        float ds = os * (fs - base);
+        float da = oa * (fa - odd);
+        if (forced) {
+            const float cg = float(L::cx(q)) * g[0] + float(L::cy(q)) * g[1] + float(L::cz(q)) * g[2];
+            ds -= ps * L::w(q) * rho * (-3.0f * ug + 9.0f * cu * cg);
+            da -= pa * L::w(q) * rho * (3.0f * cg);
+        }
         f[q] = f[q] - ds - da;
         f[o] = f[o] - ds + da;
     }
+}
+
+// Body-force terms only when a force is set: the unforced form saves the
+// per-pair force arithmetic in the common case (uniform branch).
+template <int Q>
+__device__ __forceinline__ void collide_trt(float* f, float rho, const float u[3], const float g[3], float tau_s,
+                                            float tau_a) {
+    if (g[0] != 0.0f || g[1] != 0.0f || g[2] != 0.0f) collide_trt_t<Q>(f, rho, u, g, tau_s, tau_a, true);
+    else collide_trt_t<Q>(f, rho, u, g, tau_s, tau_a, false);
 }
 
 // The reference's D3Q27 "opposite" table (include/wake/ispc/lbm_d3q27.isph:35-40):

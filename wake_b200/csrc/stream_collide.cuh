@@ -301,23 +301,40 @@ __global__ void __launch_bounds__(256, 4) k_step_fast(const StepArgs a) {
     using C = Codec<S>;
     using T = typename C::T;
     const unsigned e = a.rows[blockIdx.x];
+    const int nx = a.geo.nx, ny = a.geo.ny, nz = a.geo.nz;
     const int y = static_cast<int>(e & 0xffffu), z = static_cast<int>(e >> 16);
-    const long long row0 = (static_cast<long long>(z) * a.geo.ny + y) * a.geo.nx;
-    const T* fin = static_cast<const T*>(a.fin);
-    T* out = static_cast<T*>(a.fout);
-    for (int x = threadIdx.x; x < a.geo.nx; x += blockDim.x) {
-        const long long i = row0 + x;
-        const uint8_t fl = a.flags[i];
+    const long long row0 = (static_cast<long long>(z) * ny + y) * nx;
+    // Source-row offsets of the (cy, cz) shifts relative to this row, y / z wraps
+    // applied: uniform across the block, so with the plane offsets they form
+    // warp-uniform address terms and each load is a per-thread base plus a uniform offset.
+    const int yl = (y + 1 == ny) ? (a.geo.periodic_y ? 0 : y + 1) : y + 1;  // source row for cy = -1
+    const int yh = (y == 0) ? (a.geo.periodic_y ? ny - 1 : -1) : y - 1;     // source row for cy = +1
+    const int zl = (z + 1 == nz) ? (a.geo.periodic_z ? 0 : z + 1) : z + 1;
+    const int zh = (z == 0) ? (a.geo.periodic_z ? nz - 1 : -1) : z - 1;
+    const int ysrc[3] = {yl, y, yh}, zsrc[3] = {zl, z, zh};
+    const T* fin = static_cast<const T*>(a.fin) + row0;
+    T* out = static_cast<T*>(a.fout) + row0;
+    const long long P = a.geo.pitch;
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+        const uint8_t fl = a.flags[row0 + x];
+        // the three per-thread bases: source x for cx = -1, 0, +1 (periodic in x)
+        const T* b[3] = {fin + (x + 1 == nx ? 0 : x + 1), fin + x, fin + (x == 0 ? nx - 1 : x - 1)};
         float f[Q];
-        gather_pure<Q, S>(fin, a.geo, x, y, z, f);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const long long rowoff =
+                (static_cast<long long>(zsrc[L::cz(q) + 1] - z) * ny + (ysrc[L::cy(q) + 1] - y)) * nx;
+            f[q] = C::load(b[L::cx(q) + 1] + (q * P + rowoff), L::w(q));
+        }
         if (fl & FL_ZH_IN) zou_he_inlet<Q>(f, a.geo.uin);
         if (fl & FL_ZH_OUT) zou_he_outlet<Q>(f, a.geo.rho_out);
         float rho, u[3];
         node_moments<Q>(f, a.phys.g, rho, u);
         if (!(rho > 0.0f) || !(fabsf(u[0]) < 1e30f)) atomicOr(a.status, ERR_NONFINITE);
         collide<Q, COLL, LES>(f, rho, u, a.phys);
+        T* o = out + x;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) C::store_stream(out + q * a.geo.pitch + i, f[q], L::w(q));
+        for (int q = 0; q < Q; ++q) C::store_stream(o + q * P, f[q], L::w(q));
     }
 }
 
