@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--graph", type=int, default=20, help="steps per captured CUDA graph (0: plain launches)")
     p.add_argument("--profile", choices=["f32", "f16", "bf16"], default=None,
                    help="profiling mode: only warm-up + timed steps of this storage, plain launches, one JSON line")
+    p.add_argument("--block", type=int, default=0, help="threads per block of the fused step (0: automatic)")
     return p.parse_args()
 
 
@@ -58,11 +59,17 @@ def run_profile(args):
 
     from wake_b200 import workloads as W
 
+    import wake_b200 as wb
+
     case = W.sphere_channel()
     g = W.build_grid(case, storage=args.profile)
+    if args.block:
+        wb.check(wb.lib.wake_grid_set_block(g.handle, args.block))
+    if args.graph:
+        g.use_graph(args.graph)
     ms = timed_steps(g, case, args.steps, args.warmup, 1)
-    print(json.dumps({"profile": args.profile, "steps": args.steps, "ms_per_step": ms / args.steps,
-                      "mlups": case.n * args.steps / (ms * 1e-3) / 1e6}))
+    print(json.dumps({"profile": args.profile, "block": wb.lib.wake_grid_get_block(g.handle), "steps": args.steps,
+                      "ms_per_step": ms / args.steps, "mlups": case.n * args.steps / (ms * 1e-3) / 1e6}))
     torch.cuda.synchronize()
 
 

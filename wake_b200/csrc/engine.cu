@@ -134,6 +134,33 @@ __global__ void k_diag_partials(const float* __restrict__ rho, const float* __re
         for (int c = 0; c < 4; ++c) part[4 * blockIdx.x + c] = s[c][0];
 }
 
+// Sum the per-node momentum-exchange contributions of one step in slot order
+// (one block: thread t takes slots t, t + 256, ... in order, then a fixed tree)
+// and append the force to the history. Launched after the step kernel that
+// wrote the slots, on the same stream.
+__global__ void __launch_bounds__(256) k_mem_reduce(const double* __restrict__ contrib, int n, unsigned* hist_step,
+                                                    double* hist, int hist_cap) {
+    __shared__ double red[3][256];
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int j = threadIdx.x; j < n; j += 256)
+        for (int c = 0; c < 3; ++c) s[c] += contrib[3 * static_cast<long long>(j) + c];
+    for (int c = 0; c < 3; ++c) red[c][threadIdx.x] = s[c];
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            for (int c = 0; c < 3; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const unsigned step = *hist_step;
+        double* h = hist + 3 * static_cast<long long>(step % static_cast<unsigned>(hist_cap));
+        h[0] = red[0][0];
+        h[1] = red[1][0];
+        h[2] = red[2][0];
+        *hist_step = step + 1u;
+    }
+}
+
 cudaError_t launch_link_marks(const int* link_node, int n_links, uint8_t* flags, int* node_start,
                               cudaStream_t stream) {
     if (n_links <= 0) return cudaSuccess;
@@ -178,12 +205,14 @@ struct wake_grid {
     int dev_links = 0;         // links currently on the device (the flags refer to these)
     bool links_dirty = false;  // host links differ from the device copy
 
-    int mem_on = 0, hist_cap = 0, n_slots = 0;
+    int mem_on = 0, hist_cap = 0;
     float center[3] = {0.f, 0.f, 0.f}, rmax = 0.f;
-    DevMem d_block_slot, d_partial, d_counters, d_hist;
+    DevMem d_counters, d_hist;         // counters: [0] unused, [1] history entries written
+    DevMem d_warp_base, d_contrib;     // momentum-exchange slots (see MemCfg)
+    int warps_per_row = 1, n_mem_nodes = 0;
 
     // rows handled by k_step_fast (pure-gather rows) and by k_step (the rest),
-    // packed (z << 16) | y; the k_step block of list entry b owns momentum slot block_slot[b]
+    // packed (z << 16) | y
     DevMem d_fast_rows, d_gen_rows;
     int n_fast = 0, n_gen = 0;
 
@@ -329,37 +358,50 @@ int rebuild_flags(wake_grid* g) {
         WK_CUDA(cudaMemcpyAsync(h.data(), cls.p, nr, cudaMemcpyDeviceToHost, g->stream));
         WK_CUDA(cudaStreamSynchronize(g->stream));
         std::vector<unsigned> fast, gen;
-        std::vector<int> slots;
-        int slot = 0;
+        std::vector<int> gen_row;  // row index of each general entry
         for (int r = 0; r < nr; ++r) {
             const unsigned packed = (static_cast<unsigned>(r / g->ny) << 16) | static_cast<unsigned>(r % g->ny);
-            if ((h[r] & 1) && !(g->mem_on && slot == 0 && r == nr - 1 && gen.empty())) {
+            if (h[r] & 1) {
                 fast.push_back(packed);
             } else {
                 gen.push_back(packed);
-                slots.push_back(g->mem_on && (h[r] & 2) ? slot++ : -1);
+                gen_row.push_back(r);
             }
-        }
-        if (g->mem_on && slot == 0) {
-            // no momentum-exchange link in range: one k_step block still records a zero force every step
-            slots[0] = slot++;
         }
         g->n_fast = static_cast<int>(fast.size());
         g->n_gen = static_cast<int>(gen.size());
-        g->n_slots = slot;
         WK_CUDA(g->d_fast_rows.ensure(sizeof(unsigned) * std::max<std::size_t>(1, fast.size())));
         WK_CUDA(g->d_gen_rows.ensure(sizeof(unsigned) * std::max<std::size_t>(1, gen.size())));
-        WK_CUDA(g->d_block_slot.ensure(sizeof(int) * std::max<std::size_t>(1, slots.size())));
         if (!fast.empty())
             WK_CUDA(cudaMemcpyAsync(g->d_fast_rows.p, fast.data(), sizeof(unsigned) * fast.size(),
                                     cudaMemcpyHostToDevice, g->stream));
-        if (!gen.empty()) {
+        if (!gen.empty())
             WK_CUDA(cudaMemcpyAsync(g->d_gen_rows.p, gen.data(), sizeof(unsigned) * gen.size(), cudaMemcpyHostToDevice,
                                     g->stream));
-            WK_CUDA(cudaMemcpyAsync(g->d_block_slot.p, slots.data(), sizeof(int) * slots.size(),
+        // momentum-exchange slots: per general row and 32-wide chunk, the number of
+        // FL_MEM nodes before it (node order), so slots are dense and ordered
+        g->warps_per_row = (g->nx + 31) / 32;
+        g->n_mem_nodes = 0;
+        std::vector<int> warp_base;
+        if (g->mem_on) {
+            std::vector<uint8_t> fl(g->N);
+            WK_CUDA(cudaMemcpyAsync(fl.data(), g->d_flags.p, g->N, cudaMemcpyDeviceToHost, g->stream));
+            WK_CUDA(cudaStreamSynchronize(g->stream));
+            warp_base.assign(std::max<std::size_t>(1, gen.size() * g->warps_per_row), 0);
+            int count = 0;
+            for (std::size_t e = 0; e < gen.size(); ++e) {
+                const long long row0 = static_cast<long long>(gen_row[e]) * g->nx;
+                for (int c = 0; c < g->warps_per_row; ++c) {
+                    warp_base[e * g->warps_per_row + c] = count;
+                    for (int x = 32 * c; x < std::min(g->nx, 32 * c + 32); ++x) count += (fl[row0 + x] & FL_MEM) ? 1 : 0;
+                }
+            }
+            g->n_mem_nodes = count;
+            WK_CUDA(g->d_warp_base.ensure(sizeof(int) * warp_base.size()));
+            WK_CUDA(cudaMemcpyAsync(g->d_warp_base.p, warp_base.data(), sizeof(int) * warp_base.size(),
                                     cudaMemcpyHostToDevice, g->stream));
+            WK_CUDA(g->d_contrib.ensure(sizeof(double) * 3 * std::max(1, count)));
         }
-        if (g->mem_on) WK_CUDA(g->d_partial.ensure(sizeof(double) * 3 * std::max(1, slot)));
         WK_CUDA(cudaStreamSynchronize(g->stream));  // the host vectors go out of scope
     }
     g->geom_dirty = false;
@@ -532,14 +574,13 @@ int do_steps(wake_grid* g, int n) {
             for (int c = 0; c < 3; ++c) a.mem.center[c] = g->center[c];
             a.mem.r_max = g->rmax;
             a.mem.r_max_sq = g->rmax * g->rmax;
-            a.mem.block_slot = g->d_block_slot.as<int>();
-            a.mem.partial = g->d_partial.as<double>();
-            a.mem.arrivals = g->d_counters.as<unsigned>();
+            a.mem.warp_base = g->d_warp_base.as<int>();
+            a.mem.warps_per_row = g->warps_per_row;
+            a.mem.contrib = g->d_contrib.as<double>();
+            a.mem.n_nodes = g->n_mem_nodes;
             a.mem.hist_step = g->d_counters.as<unsigned>() + 1;
             a.mem.hist = g->d_hist.as<double>();
             a.mem.hist_cap = g->hist_cap;
-            a.mem.n_slots = g->n_slots;
-            if (g->n_slots == 0) a.mem.enabled = 0;
         }
         a.phys = g->phys;
         // The pure-gather rows and the rows with boundaries / momentum exchange write
@@ -558,6 +599,12 @@ int do_steps(wake_grid* g, int n) {
             WK_CUDA(cudaStreamWaitEvent(g->side, g->ev_fork, 0));
         }
         WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, gen, side, false));
+        if (g->mem_on) {
+            // the step's force from the slots the general launch just wrote (zero if none)
+            k_mem_reduce<<<1, 256, 0, side.stream>>>(a.mem.contrib, a.mem.n_nodes, a.mem.hist_step, a.mem.hist,
+                                                     a.mem.hist_cap);
+            WK_CUDA(cudaGetLastError());
+        }
         WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, a, g->launch(), true));
         if (fork) {
             WK_CUDA(cudaEventRecord(g->ev_join, g->side));

@@ -128,8 +128,14 @@ constexpr int kQ = WK_Q;
 template <int C, int S, bool LES>
 void step_one(const StepArgs& a, const Launch& L, bool fast) {
     if (a.nrows <= 0) return;
-    if (fast) k_step_fast<kQ, C, S, LES><<<a.nrows, L.tpb_fast, 0, L.stream>>>(a);
-    else k_step<kQ, C, S, LES><<<a.nrows, L.tpb, 0, L.stream>>>(a);
+    if (fast) {
+        // 32-bit element indexing whenever every index of the state buffer fits
+        const bool idx32 = static_cast<long long>(kQ) * a.geo.pitch < (1ll << 32);
+        if (idx32) k_step_fast<kQ, C, S, LES, true><<<a.nrows, L.tpb_fast, 0, L.stream>>>(a);
+        else k_step_fast<kQ, C, S, LES, false><<<a.nrows, L.tpb_fast, 0, L.stream>>>(a);
+    } else {
+        k_step<kQ, C, S, LES><<<a.nrows, L.tpb, 0, L.stream>>>(a);
+    }
 }
 template <int C, int S, bool LES>
 void initial_one(const float* f0, void* A, void* B, const uint8_t* flags, const Geo& g, const Physics& p,

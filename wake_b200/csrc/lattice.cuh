@@ -209,6 +209,12 @@ __device__ __forceinline__ void node_moments(const float* f, const float g[3], f
 
 // Smagorinsky tau from the local non-equilibrium stress (d2q9_les.ispc:19-55,
 // d3q19_les.ispc:21-64), applied per node.
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // Because c_opp = -c, the second-order tensor only sees the even part of each
 // (q, opp) pair: Pi = sum over pairs c c^T (f_q + f_opp - 2 w rho (1 + 4.5 (c.u)^2 - 1.5 u^2)).
 // The same even parts feed the TRT update, so the compiler shares them.
@@ -233,9 +239,11 @@ __device__ __forceinline__ float smagorinsky_tau(const float* f, float rho, cons
         if (x && z) pxz += (x * z > 0) ? fn : -fn;
     }
     const float sum = pxx * pxx + pyy * pyy + pzz * pzz + 2.0f * (pxy * pxy + pyz * pyz + pxz * pxz);
-    const float qs = sqrtf(2.0f * sum);
+    // per-node relaxation time: the approximate square root and division (a few
+    // ulp) cost a fraction of the exact sequences and perturb tau by ~1e-7
+    const float qs = sqrt_approx(2.0f * sum);
     const float pref = 18.0f * 1.4142135623730951f * cs * cs;
-    return 0.5f * (tau0 + sqrtf(tau0 * tau0 + (pref / rho) * qs));
+    return 0.5f * (tau0 + sqrt_approx(tau0 * tau0 + __fdividef(pref, rho) * qs));
 }
 
 template <int Q>
@@ -254,10 +262,9 @@ __device__ __forceinline__ void collide_bgk(float* f, float rho, const float u[3
 }
 
 template <int Q>
-__device__ __forceinline__ void collide_trt_t(float* f, float rho, const float u[3], const float g[3], float tau_s,
-                                              float tau_a, bool forced) {
+__device__ __forceinline__ void collide_trt_t(float* f, float rho, const float u[3], const float g[3], float os,
+                                              float oa, bool forced) {
     using L = Lat<Q>;
-    const float os = 1.0f / tau_s, oa = 1.0f / tau_a;
     const float ps = 1.0f - 0.5f * os, pa = 1.0f - 0.5f * oa;
     const float u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
     const float ug = forced ? u[0] * g[0] + u[1] * g[1] + u[2] * g[2] : 0.0f;
@@ -287,13 +294,115 @@ __device__ __forceinline__ void collide_trt_t(float* f, float rho, const float u
     }
 }
 
+// Index of the direction that starts pair p (the member whose opposite is larger).
+template <int Q>
+__host__ __device__ constexpr int pair_q(int p) {
+    int seen = 0;
+    for (int q = 1; q < Q; ++q) {
+        if (Lat<Q>::opp(q) < q) continue;
+        if (seen == p) return q;
+        ++seen;
+    }
+    return 0;
+}
+
+// Moments, Smagorinsky tau (LES) and TRT relaxation in one pass over the pair
+// sums s = f_q + f_opp and differences d = f_q - f_opp, which all three share:
+// rho = f_0 + sum s, j = sum c d, Pi = sum c c^T (s - 2 even(feq)), and the TRT
+// update relaxes s/2 to the even and d/2 to the odd part of feq. Writes the
+// post-collision populations back into f and the (Guo-shifted) moments.
+template <int Q, bool LES>
+__device__ __forceinline__ void trt_pairs(float* f, const Physics& P, float& rho, float u[3]) {
+    using L = Lat<Q>;
+    constexpr int NP = (Q - 1) / 2;
+    float s[NP], d[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        const int q = pair_q<Q>(p), o = L::opp(q);
+        s[p] = f[q] + f[o];
+        d[p] = f[q] - f[o];
+    }
+    float r = f[0], jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        const int q = pair_q<Q>(p);
+        r += s[p];
+        if (L::cx(q)) jx += L::cx(q) > 0 ? d[p] : -d[p];
+        if (L::cy(q)) jy += L::cy(q) > 0 ? d[p] : -d[p];
+        if (L::cz(q)) jz += L::cz(q) > 0 ? d[p] : -d[p];
+    }
+    rho = r;
+    const float inv = 1.0f / r;
+    const float* g = P.g;
+    u[0] = (jx + 0.5f * r * g[0]) * inv;
+    u[1] = (jy + 0.5f * r * g[1]) * inv;
+    u[2] = (jz + 0.5f * r * g[2]) * inv;
+    const float u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const float a0 = 1.0f - 1.5f * u2;
+    float os, oa;
+    if (LES) {
+        float pxx = 0.f, pyy = 0.f, pzz = 0.f, pxy = 0.f, pyz = 0.f, pxz = 0.f;
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const int q = pair_q<Q>(p);
+            const int x = L::cx(q), y = L::cy(q), z = L::cz(q);
+            const float cu = float(x) * u[0] + float(y) * u[1] + float(z) * u[2];
+            const float fn = s[p] - 2.0f * (L::w(q) * r * (a0 + 4.5f * cu * cu));
+            if (x) pxx += fn;
+            if (y) pyy += fn;
+            if (z) pzz += fn;
+            if (x && y) pxy += (x * y > 0) ? fn : -fn;
+            if (y && z) pyz += (y * z > 0) ? fn : -fn;
+            if (x && z) pxz += (x * z > 0) ? fn : -fn;
+        }
+        const float sum = pxx * pxx + pyy * pyy + pzz * pzz + 2.0f * (pxy * pxy + pyz * pyz + pxz * pxz);
+        const float pref = 18.0f * 1.4142135623730951f * P.cs_smag * P.cs_smag;
+        const float tau = 0.5f * (P.tau + sqrt_approx(P.tau * P.tau + __fdividef(pref, r) * sqrt_approx(2.0f * sum)));
+        const float tau_a = 0.5f + __fdividef(P.lambda_trt, fmaxf(1e-4f, tau - 0.5f));
+        os = __fdividef(1.0f, tau);
+        oa = __fdividef(1.0f, tau_a);
+    } else {
+        const float tau_a = 0.5f + P.lambda_trt / fmaxf(1e-4f, P.tau - 0.5f);
+        os = 1.0f / P.tau;
+        oa = 1.0f / tau_a;
+    }
+    const bool forced = (g[0] != 0.0f) || (g[1] != 0.0f) || (g[2] != 0.0f);
+    const float ps = 1.0f - 0.5f * os, pa = 1.0f - 0.5f * oa;
+    const float ug = u[0] * g[0] + u[1] * g[1] + u[2] * g[2];
+    f[0] = f[0] - os * (f[0] - L::w(0) * r * a0);
+    if (forced) f[0] += ps * L::w(0) * r * (-3.0f * ug);
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        const int q = pair_q<Q>(p), o = L::opp(q);
+        const float cu = float(L::cx(q)) * u[0] + float(L::cy(q)) * u[1] + float(L::cz(q)) * u[2];
+        const float wr = L::w(q) * r;
+        float ds = os * (0.5f * s[p] - wr * (a0 + 4.5f * cu * cu));
+        float da = oa * (0.5f * d[p] - 3.0f * wr * cu);
+        if (forced) {
+            const float cg = float(L::cx(q)) * g[0] + float(L::cy(q)) * g[1] + float(L::cz(q)) * g[2];
+            ds -= ps * wr * (-3.0f * ug + 9.0f * cu * cg);
+            da -= pa * wr * (3.0f * cg);
+        }
+        // f_q = (s + d)/2 - ds - da, f_opp = (s - d)/2 - ds + da
+        const float hs = 0.5f * s[p] - ds, hd = 0.5f * d[p] - da;
+        f[q] = hs + hd;
+        f[o] = hs - hd;
+    }
+}
+
 // Body-force terms only when a force is set: the unforced form saves the
 // per-pair force arithmetic in the common case (uniform branch).
 template <int Q>
+__device__ __forceinline__ void collide_trt_omega(float* f, float rho, const float u[3], const float g[3], float os,
+                                                  float oa) {
+    if (g[0] != 0.0f || g[1] != 0.0f || g[2] != 0.0f) collide_trt_t<Q>(f, rho, u, g, os, oa, true);
+    else collide_trt_t<Q>(f, rho, u, g, os, oa, false);
+}
+
+template <int Q>
 __device__ __forceinline__ void collide_trt(float* f, float rho, const float u[3], const float g[3], float tau_s,
                                             float tau_a) {
-    if (g[0] != 0.0f || g[1] != 0.0f || g[2] != 0.0f) collide_trt_t<Q>(f, rho, u, g, tau_s, tau_a, true);
-    else collide_trt_t<Q>(f, rho, u, g, tau_s, tau_a, false);
+    collide_trt_omega<Q>(f, rho, u, g, 1.0f / tau_s, 1.0f / tau_a);
 }
 
 // The reference's D3Q27 "opposite" table (include/wake/ispc/lbm_d3q27.isph:35-40):
@@ -609,8 +718,14 @@ __device__ __forceinline__ void collide(float* f, float rho, const float u[3], c
         collide_bgk<Q>(f, rho, u, P.g, tau);
     } else if (COLL == COLL_TRT) {
         // tau_a from the magic parameter (lattice_grid_2d.cpp:219-222)
-        const float tau_a = 0.5f + P.lambda_trt / fmaxf(1e-4f, tau - 0.5f);
-        collide_trt<Q>(f, rho, u, P.g, tau, tau_a);
+        if (LES) {
+            // per-node rates: approximate divisions (see smagorinsky_tau)
+            const float tau_a = 0.5f + __fdividef(P.lambda_trt, fmaxf(1e-4f, tau - 0.5f));
+            collide_trt_omega<Q>(f, rho, u, P.g, __fdividef(1.0f, tau), __fdividef(1.0f, tau_a));
+        } else {
+            const float tau_a = 0.5f + P.lambda_trt / fmaxf(1e-4f, tau - 0.5f);
+            collide_trt<Q>(f, rho, u, P.g, tau, tau_a);
+        }
     } else {
         if constexpr (Q == 9) collide_mrt_d2q9(f, rho, u, P.g, tau, P.tau_bulk);
         else if constexpr (Q == 19) collide_mrt_d3q19(f, rho, u, P.g, tau, P.tau_bulk, P.mrt_exact);

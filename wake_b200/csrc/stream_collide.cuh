@@ -44,13 +44,17 @@ struct MemCfg {                   // momentum-exchange monitor
     int enabled;
     float center[3];
     float r_max, r_max_sq;
-    const int* block_slot;        // [grid] slot of the block's partial, -1 if none
-    double* partial;              // [n_slots][3]
-    unsigned* arrivals;           // block arrival counter (reset by the last block)
+    // Every node carrying FL_MEM owns one fixed slot of `contrib`, numbered in node
+    // order: slot = warp_base[entry * warps_per_row + x / 32] + (rank of the node
+    // among the FL_MEM nodes of its 32-wide chunk). k_mem_reduce sums the slots in
+    // slot order, so the force is reproducible bit for bit and needs no barrier.
+    const int* warp_base;         // [general rows][warps_per_row]
+    int warps_per_row;
+    double* contrib;              // [n_nodes][3]
+    int n_nodes;
     unsigned* hist_step;          // number of entries written so far
     double* hist;                 // [hist_cap][3]: (Fx, Fy, Tz) in 2D, (Fx, Fy, Fz) in 3D
     int hist_cap;
-    int n_slots;
 };
 
 struct Out {                      // optional outputs of the materialise kernel
@@ -203,48 +207,6 @@ __device__ __forceinline__ void mem_node(const float* f, unsigned bb, int x, int
     }
 }
 
-// Deterministic block reduction of the momentum exchange: each contributing block
-// writes its partial to a fixed slot; the last block to arrive sums the slots in
-// slot order and appends the step's force to the history. No waiting: arrival is
-// counted with one atomic, the last arriver does the final sum.
-__device__ __forceinline__ void mem_block_finish(const MemCfg& M, double acc[3], int slot) {
-    __shared__ double red[3][32];
-    __shared__ bool last;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        double v = acc[c];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (lane == 0) red[c][warp] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double s[3] = {0.0, 0.0, 0.0};
-        for (int w = 0; w < nw; ++w)
-            for (int c = 0; c < 3; ++c) s[c] += red[c][w];
-        for (int c = 0; c < 3; ++c) M.partial[3 * slot + c] = s[c];
-        __threadfence();
-        const unsigned prev = atomicAdd(M.arrivals, 1u);
-        last = (prev == static_cast<unsigned>(M.n_slots) - 1u);
-    }
-    __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
-        double s[3] = {0.0, 0.0, 0.0};
-        const volatile double* p = M.partial;
-        for (int k = 0; k < M.n_slots; ++k)
-            for (int c = 0; c < 3; ++c) s[c] += p[3 * k + c];
-        const unsigned step = *M.hist_step;
-        double* h = M.hist + 3 * static_cast<long long>(step % static_cast<unsigned>(M.hist_cap));
-        h[0] = s[0];
-        h[1] = s[1];
-        h[2] = s[2];
-        *M.hist_step = step + 1u;
-        *M.arrivals = 0u;
-    }
-}
-
 struct StepArgs {
     const void* fin;
     void* fout;
@@ -269,33 +231,48 @@ __global__ void __launch_bounds__(512) k_step(const StepArgs a) {
     const unsigned e = a.rows[blockIdx.x];
     const int y = static_cast<int>(e & 0xffffu), z = static_cast<int>(e >> 16);
     const long long row0 = (static_cast<long long>(z) * a.geo.ny + y) * a.geo.nx;
-    double acc[3] = {0.0, 0.0, 0.0};
-    for (int x = threadIdx.x; x < a.geo.nx; x += blockDim.x) {
+    const int nx = a.geo.nx, lane = threadIdx.x & 31;
+    // warps walk the row in 32-wide chunks (x = chunk + lane)
+    for (int xb = threadIdx.x - lane; xb < nx; xb += blockDim.x) {
+        const int x = xb + lane;
+        if (x >= nx) continue;
         const long long i = row0 + x;
         const uint8_t fl = a.flags[i];
+        int slot = -1;
+        if (a.mem.enabled) {
+            // slot = chunk base + rank among this chunk's momentum-exchange nodes
+            const unsigned live = (nx - xb >= 32) ? 0xffffffffu : ((1u << (nx - xb)) - 1u);
+            const bool m = (fl & FL_MEM) != 0;
+            const unsigned bal = __ballot_sync(live, m);
+            if (m) slot = a.mem.warp_base[blockIdx.x * a.mem.warps_per_row + (xb >> 5)] +
+                          __popc(bal & ((1u << lane) - 1u));
+        }
         if ((fl & FL_TYPE) == CT_SOLID) continue;
         float f[Q];
         unsigned bb;
         gather<Q, S>(static_cast<const T*>(a.fin), a.geo, a.flags, a.links, x, y, z, i, fl, f, bb);
         float rho, u[3];
         node_moments<Q>(f, a.phys.g, rho, u);
-        if (fl & FL_MEM) mem_node<Q>(f, bb, x, y, z, a.geo, a.mem, acc);
+        if (slot >= 0) {
+            double acc[3] = {0.0, 0.0, 0.0};
+            mem_node<Q>(f, bb, x, y, z, a.geo, a.mem, acc);
+            double* c = a.mem.contrib + 3 * static_cast<long long>(slot);
+            c[0] = acc[0];
+            c[1] = acc[1];
+            c[2] = acc[2];
+        }
         if (!(rho > 0.0f) || !(fabsf(u[0]) < 1e30f)) atomicOr(a.status, ERR_NONFINITE);
         collide<Q, COLL, LES>(f, rho, u, a.phys);
         T* out = static_cast<T*>(a.fout);
 #pragma unroll
         for (int q = 0; q < Q; ++q) C::store_stream(out + q * a.geo.pitch + i, f[q], L::w(q));
     }
-    if (a.mem.enabled) {
-        const int slot = a.mem.block_slot[blockIdx.x];
-        if (slot >= 0) mem_block_finish(a.mem, acc, slot);
-    }
 }
 
 // The same step for rows whose every node is a pure gather (no solid, no
 // bounce-back, no curved link; Zou-He allowed) -- the bulk of a domain. Without
 // the rare paths the kernel fits 64 registers, i.e. four 256-thread blocks per SM.
-template <int Q, int COLL, int S, bool LES>
+template <int Q, int COLL, int S, bool LES, bool IDX32>
 __global__ void __launch_bounds__(256, 4) k_step_fast(const StepArgs a) {
     using L = Lat<Q>;
     using C = Codec<S>;
@@ -312,29 +289,49 @@ __global__ void __launch_bounds__(256, 4) k_step_fast(const StepArgs a) {
     const int zl = (z + 1 == nz) ? (a.geo.periodic_z ? 0 : z + 1) : z + 1;
     const int zh = (z == 0) ? (a.geo.periodic_z ? nz - 1 : -1) : z - 1;
     const int ysrc[3] = {yl, y, yh}, zsrc[3] = {zl, z, zh};
-    const T* fin = static_cast<const T*>(a.fin) + row0;
-    T* out = static_cast<T*>(a.fout) + row0;
-    const long long P = a.geo.pitch;
+    const T* fin = static_cast<const T*>(a.fin);
+    T* out = static_cast<T*>(a.fout);
     for (int x = threadIdx.x; x < nx; x += blockDim.x) {
         const uint8_t fl = a.flags[row0 + x];
-        // the three per-thread bases: source x for cx = -1, 0, +1 (periodic in x)
-        const T* b[3] = {fin + (x + 1 == nx ? 0 : x + 1), fin + x, fin + (x == 0 ? nx - 1 : x - 1)};
+        // source x for cx = -1, 0, +1 (periodic in x)
+        const int xs[3] = {x + 1 == nx ? 0 : x + 1, x, x == 0 ? nx - 1 : x - 1};
         float f[Q];
+        if constexpr (IDX32) {
+            // element index in 32-bit unsigned arithmetic (Q * pitch < 2^32): the
+            // plane + source-row part is uniform, each access adds x and scales once
+            const unsigned P = static_cast<unsigned>(a.geo.pitch);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const long long rowoff =
-                (static_cast<long long>(zsrc[L::cz(q) + 1] - z) * ny + (ysrc[L::cy(q) + 1] - y)) * nx;
-            f[q] = C::load(b[L::cx(q) + 1] + (q * P + rowoff), L::w(q));
+            for (int q = 0; q < Q; ++q) {
+                const unsigned rowsrc = static_cast<unsigned>((zsrc[L::cz(q) + 1] * ny + ysrc[L::cy(q) + 1]) * nx);
+                f[q] = C::load(fin + (q * P + rowsrc + static_cast<unsigned>(xs[L::cx(q) + 1])), L::w(q));
+            }
+        } else {
+            const long long P = a.geo.pitch;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const long long rowsrc = (static_cast<long long>(zsrc[L::cz(q) + 1]) * ny + ysrc[L::cy(q) + 1]) * nx;
+                f[q] = C::load(fin + (q * P + rowsrc + xs[L::cx(q) + 1]), L::w(q));
+            }
         }
         if (fl & FL_ZH_IN) zou_he_inlet<Q>(f, a.geo.uin);
         if (fl & FL_ZH_OUT) zou_he_outlet<Q>(f, a.geo.rho_out);
         float rho, u[3];
-        node_moments<Q>(f, a.phys.g, rho, u);
+        if constexpr (COLL == COLL_TRT) {
+            trt_pairs<Q, LES>(f, a.phys, rho, u);
+        } else {
+            node_moments<Q>(f, a.phys.g, rho, u);
+            collide<Q, COLL, LES>(f, rho, u, a.phys);
+        }
         if (!(rho > 0.0f) || !(fabsf(u[0]) < 1e30f)) atomicOr(a.status, ERR_NONFINITE);
-        collide<Q, COLL, LES>(f, rho, u, a.phys);
-        T* o = out + x;
+        if constexpr (IDX32) {
+            const unsigned P = static_cast<unsigned>(a.geo.pitch), i = static_cast<unsigned>(row0 + x);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) C::store_stream(o + q * P, f[q], L::w(q));
+            for (int q = 0; q < Q; ++q) C::store_stream(out + (q * P + i), f[q], L::w(q));
+        } else {
+            const long long P = a.geo.pitch, i = row0 + x;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) C::store_stream(out + (q * P + i), f[q], L::w(q));
+        }
     }
 }
 
