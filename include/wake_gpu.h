@@ -252,6 +252,15 @@ void* wake_grid_state_buffer(wake_grid* g, int which);
 /* Launch shape of the fused kernel: threads per block (32..512, multiple of 32). */
 int wake_grid_set_block(wake_grid* g, int threads_per_block);
 int wake_grid_get_block(wake_grid* g);
+/* Kernel launches one fused step issues with the current geometry (pure-gather
+ * rows, general rows, momentum-exchange reduction). No reference counterpart. */
+int wake_grid_launches_per_step(wake_grid* g);
+/* CUDA-event timing of each pure-gather (bulk) launch. While on, steps run as
+ * plain launches (no graph). bulk_launch_times synchronizes, returns the summed
+ * duration of the launches recorded since the last read, their count and the
+ * nodes one launch updates, and restarts the count. No reference counterpart. */
+int wake_grid_time_bulk_launches(wake_grid* g, int on);
+int wake_grid_bulk_launch_times(wake_grid* g, double* total_ms, long long* launches, long long* nodes_per_launch);
 
 /* FP64 Strouhal frequency of a lift history (strouhal_analyzer.cpp:39-84:
  * mean removed, Hann window over the first min(n, 4096) samples, radix-2 FFT,

@@ -231,8 +231,14 @@ struct wake_grid {
     float graph_g[3] = {0.f, 0.f, 0.f};
     bool graph_ok = false;
 
+    // Optional CUDA-event timing of every pure-gather (bulk) launch; plain launches only.
+    bool time_bulk = false;
+    std::vector<cudaEvent_t> t_ev;  // pairs (start, end), reused
+    std::size_t t_used = 0;         // events recorded since the last read
+
     explicit wake_grid(int q) : lat(q) {}
     ~wake_grid() {
+        for (cudaEvent_t e : t_ev) cudaEventDestroy(e);
         if (graph) cudaGraphExecDestroy(graph);
         if (own_stream && stream) cudaStreamDestroy(stream);
         if (side) cudaStreamDestroy(side);
@@ -293,10 +299,12 @@ struct wake_grid {
         }
         xchunks = (nx + tpb - 1) / tpb;
         rows = ny * nz;
-        // k_step_fast is limited to 256 threads (four blocks per SM): least idle lanes over the row
+        // k_step_fast is limited to 256 threads (four blocks per SM). Least idle lanes over the row,
+        // ties to the smaller block: 64-thread blocks measured fastest on 256-node rows (more
+        // independent blocks in flight per SM, shorter tail per row).
         const int cap = std::min(want > 0 ? want : 256, 256);
         int best = -1, best_waste = 1 << 30;
-        for (int t = cap; t >= 64; t -= 32) {
+        for (int t = 64; t <= cap; t += 32) {
             const int waste = ((nx + t - 1) / t) * t - nx;
             if (waste < best_waste) {
                 best = t;
@@ -605,7 +613,20 @@ int do_steps(wake_grid* g, int n) {
                                                      a.mem.hist_cap);
             WK_CUDA(cudaGetLastError());
         }
+        const bool timed = g->time_bulk && a.nrows > 0;
+        if (timed) {
+            while (g->t_ev.size() < g->t_used + 2) {
+                cudaEvent_t e = nullptr;
+                WK_CUDA(cudaEventCreate(&e));
+                g->t_ev.push_back(e);
+            }
+            WK_CUDA(cudaEventRecord(g->t_ev[g->t_used], g->stream));
+        }
         WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, a, g->launch(), true));
+        if (timed) {
+            WK_CUDA(cudaEventRecord(g->t_ev[g->t_used + 1], g->stream));
+            g->t_used += 2;
+        }
         if (fork) {
             WK_CUDA(cudaEventRecord(g->ev_join, g->side));
             WK_CUDA(cudaStreamWaitEvent(g->stream, g->ev_join, 0));
@@ -1026,7 +1047,7 @@ int wake_grid_step(wake_grid* g, int n, float gx, float gy, float gz) {
     int r = prepare(g);
     if (r) return r;
     int done = 0;
-    if (g->graph_steps > 0 && n >= g->graph_steps) {
+    if (g->graph_steps > 0 && n >= g->graph_steps && !g->time_bulk) {
         // (re)capture a graph of graph_steps launches from the current parity
         const int gs = g->graph_steps;
         if (!g->graph_ok || g->graph_cur != g->cur) {
@@ -1174,5 +1195,36 @@ int wake_grid_set_block(wake_grid* g, int threads_per_block) {
 }
 
 int wake_grid_get_block(wake_grid* g) { return g ? g->tpb : WAKE_ERR_INVALID; }
+
+int wake_grid_launches_per_step(wake_grid* g) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    const int r = prepare(g);
+    if (r) return r;
+    return (g->n_fast > 0 ? 1 : 0) + (g->n_gen > 0 ? 1 : 0) + (g->mem_on ? 1 : 0);
+}
+
+int wake_grid_time_bulk_launches(wake_grid* g, int on) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    g->time_bulk = on != 0;
+    g->t_used = 0;
+    return WAKE_OK;
+}
+
+int wake_grid_bulk_launch_times(wake_grid* g, double* total_ms, long long* launches, long long* nodes_per_launch) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    double sum = 0.0;
+    for (std::size_t i = 0; i + 1 < g->t_used; i += 2) {
+        float ms = 0.f;
+        WK_CUDA(cudaEventElapsedTime(&ms, g->t_ev[i], g->t_ev[i + 1]));
+        sum += ms;
+    }
+    if (total_ms) *total_ms = sum;
+    if (launches) *launches = static_cast<long long>(g->t_used / 2);
+    if (nodes_per_launch) *nodes_per_launch = static_cast<long long>(g->n_fast) * g->nx;
+    g->t_used = 0;
+    return WAKE_OK;
+}
 
 }  // extern "C"
