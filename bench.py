@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--no-fp16", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-batch", action="store_true", help="skip the batched ellipse-sweep leg")
+    p.add_argument("--batch-only", action="store_true", help="only the batched ellipse-sweep leg (one JSON line)")
     p.add_argument("--graph", type=int, default=20, help="steps per captured CUDA graph (0: plain launches)")
     p.add_argument("--profile", choices=["f32", "f16", "bf16"], default=None,
                    help="profiling mode: only warm-up + timed steps of this storage, plain launches, one JSON line")
@@ -221,6 +223,93 @@ def bulk_kernel_time(g, case, steps):
     return tot.value / max(1, cnt.value), nodes.value
 
 
+BATCH_WORKLOAD = ("batched D2Q9 TRT(Lambda=1/4)+Smagorinsky(Cs=0.17) ellipse sweep: 512 domains, NX~U[64,512], NY=NX/2, semi-axes in [NY/16,NY/6], "
+                  "aspect in [1,3], angle of attack in [0,20] deg, Re in [50,300], inlet u=0.05, 5000 steps each")
+STEPS_PER_SIM = 5000
+
+
+def batched_leg(storage, n_domains=512, steps=STEPS_PER_SIM, warmup=20, baseline_jobs=16):
+    """Sims/s of the ellipse sweep advanced as one batch, and of the same jobs launched per job.
+
+    Batched: every domain resident, one bulk + one general launch + one force
+    reduction per step for all 512 domains, CUDA graphs of 20 steps, bulk block
+    size from the autotuner. Per job: the first `baseline_jobs` domains run one
+    after another through their own grid with plain launches (the single-lattice
+    API used once per job). Both time `steps` steps with CUDA events after warm-up;
+    setup is outside both timed regions."""
+    import torch
+
+    import wake_b200 as wb
+    from wake_b200 import workloads as W
+    from wake_b200.batch import Batch
+
+    cases = W.ellipse_sweep(n_domains)
+    nodes = sum(c.n for c in cases)
+    stream = torch.cuda.Stream()
+    b = Batch(9, storage)
+    b.set_stream(stream.cuda_stream)
+    grids = []
+    for c in cases:
+        g = W.build_grid(c, storage=storage)
+        b.add(g, c.collision, use_les=c.les, smag_const=c.cs_smag)
+        grids.append(g)
+    b.step(1)
+    b.synchronize()
+    for g in grids:
+        wb.check(wb.lib.wake_grid_release_scratch(g.handle))
+    best = b.autotune(steps=10)
+    b.use_graph(20)
+    b.step(warmup)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    b.step(steps)
+    t1.record(stream)
+    t1.synchronize()
+    ms = t0.elapsed_time(t1)
+    info = b.info()
+    unstable = 0
+    for g in grids:
+        try:
+            g.synchronize()
+        except wb.WakeError:
+            unstable += 1
+    b.close()
+    for g in grids:
+        g.close()
+    del grids
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+
+    # per-job plain launches on the same jobs' first `baseline_jobs` domains
+    per_job_ms = 0.0
+    base_nodes = 0
+    for c in cases[:baseline_jobs]:
+        g = W.build_grid(c, storage=storage)
+        g.set_stream(stream.cuda_stream)
+        g.step(c.collision, use_les=c.les, smag_const=c.cs_smag, n=warmup)
+        g.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.step(c.collision, use_les=c.les, smag_const=c.cs_smag, n=steps)
+        e1.record(stream)
+        e1.synchronize()
+        per_job_ms += e0.elapsed_time(e1)
+        base_nodes += c.n
+        g.close()
+    bpn = 2 * 9 * (4 if storage == "f32" else 2) + 1
+    sims = n_domains * steps / STEPS_PER_SIM / (ms * 1e-3)
+    base_sims = baseline_jobs * steps / STEPS_PER_SIM / (per_job_ms * 1e-3)
+    return {"metric": "sims/s", "value": sims, "unit": "sims/s", "storage": storage, "domains": n_domains,
+            "nodes": nodes, "steps": steps, "ms_per_step": ms / steps, "mlups": nodes * steps / (ms * 1e-3) / 1e6,
+            "achieved_gbs": bpn * nodes * steps / (ms * 1e-3) / 1e9, "bytes_per_node": bpn,
+            "bulk_block": best, "bulk_rows": info["bulk_rows"], "general_rows": info["general_rows"],
+            "launches_per_step": info["launches_per_step"], "unstable_members": unstable,
+            "per_job_plain": {"value": base_sims, "unit": "sims/s", "jobs": baseline_jobs,
+                              "mlups": base_nodes * steps / (per_job_ms * 1e-3) / 1e6},
+            "speedup_vs_per_job": sims / base_sims}
+
+
 def reference_sample(case_ref, steps_cap, budget_s, threads=1):
     """Time the reference's own LatticeGrid3D::step + momentum exchange (oracle/_ref) on host cores."""
     import oracle
@@ -297,6 +386,10 @@ def main():
         return
     if args.profile:
         run_profile(args)
+        return
+    if args.batch_only:
+        out = {"workload": BATCH_WORKLOAD, "f32": batched_leg("f32"), "f16": batched_leg("f16")}
+        print(json.dumps(out))
         return
     world, rank, local = dist_setup(args)
     import torch
@@ -381,6 +474,9 @@ def main():
                "job": "H2D of the initial populations from pinned host memory, K fused steps through "
                       "wake_grid_step, D2H of the per-step force history and of rho/u/speed"}
         del g
+    batched = None
+    if not args.no_batch:
+        batched = {"workload": BATCH_WORKLOAD, "f32": batched_leg("f32"), "f16": batched_leg("f16")}
     clocks.stop()
 
     # ---- CPU baseline (rank 0, N = 1)
@@ -400,7 +496,8 @@ def main():
                            "l2": "inputs larger than L2 (two 319 MB population buffers, 126 MB L2)",
                            "parallelism": "replicas" if world > 1 else "single GPU",
                            "graph_steps": args.graph, "final_cd": cd},
-                "roofline": roof, "fp16": fp16, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
+                "roofline": roof, "fp16": fp16, "cpu_baseline": cpu, "e2e": e2e, "batched": batched,
+                "clocks": clocks.summary(),
                 "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line))
     if world > 1:

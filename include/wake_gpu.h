@@ -262,6 +262,50 @@ int wake_grid_launches_per_step(wake_grid* g);
 int wake_grid_time_bulk_launches(wake_grid* g, int on);
 int wake_grid_bulk_launch_times(wake_grid* g, double* total_ms, long long* launches, long long* nodes_per_launch);
 
+/* Rotated solid ellipse, semi-axes a (along the rotated x axis) and b, angle in
+ * radians; extruded along z in 3D. Cell-centre test in float like
+ * GeometryPrimitives::voxelize_ellipsoid (src/geometry/primitives.cpp:73-99),
+ * which has no rotation and no 2D form. */
+int wake_grid_set_solid_ellipse(wake_grid* g, float cx, float cy, float a, float b, float angle);
+
+/* Device memory: what the grid holds now, and an upper estimate for a new grid
+ * of that shape (state buffers, FP32 initialisation scratch, flags, tables and,
+ * with with_fields, the macroscopic-field scratch). release_scratch frees the
+ * FP32 population and field scratch (re-allocated on demand by the readers).
+ * No reference counterpart (the reference allocates host AlignedBuffers,
+ * include/wake/core/memory.hpp:52-159). */
+long long wake_grid_device_bytes(wake_grid* g);
+long long wake_grid_estimate_bytes(int q, int nx, int ny, int nz, int storage, int with_fields);
+int wake_grid_release_scratch(wake_grid* g);
+
+/* ------------------------------------------------------------------ batches
+ * A batch advances many resident grids together: one bulk launch over the
+ * pure-gather rows of every member, one launch over the remaining rows and one
+ * momentum-exchange reduction per step, whatever the members' sizes. Members
+ * share the lattice and storage (checked by add) and the collision model and LES
+ * switch (checked by step); sizes, tau, boundaries, geometry and force monitors
+ * are per member. A member stays an ordinary grid: its readers (populations,
+ * fields, force history, diagnostics) work between batch steps, and its results
+ * are identical to stepping it alone. Its work runs on the batch stream while it
+ * is a member. Remove a grid before destroying it. No reference counterpart:
+ * the reference steps one LatticeGrid per call (src/grid/lattice_grid_2d.cpp:195-265). */
+typedef struct wake_batch wake_batch;
+wake_batch* wake_batch_create(int q, int storage);
+void wake_batch_destroy(wake_batch* b);          /* members stay valid, back on their own streams */
+int wake_batch_add(wake_batch* b, wake_grid* g);  /* returns the member index */
+int wake_batch_remove(wake_batch* b, wake_grid* g);
+int wake_batch_size(wake_batch* b);
+int wake_batch_set_stream(wake_batch* b, void* stream);
+int wake_batch_use_graph(wake_batch* b, int steps_per_graph);
+int wake_batch_set_block(wake_batch* b, int threads_bulk, int threads_general);
+int wake_batch_get_block(wake_batch* b);
+int wake_batch_step(wake_batch* b, int n);
+int wake_batch_synchronize(wake_batch* b);        /* first member error, if any */
+int wake_batch_info(wake_batch* b, long long* nodes, int* bulk_rows, int* general_rows, int* launches_per_step);
+/* Times `steps` real steps per bulk block size (64, 128, 256) and keeps the
+ * fastest; members advance 3 * steps. Results do not depend on the choice. */
+int wake_batch_autotune(wake_batch* b, int steps, int* best_threads);
+
 /* FP64 Strouhal frequency of a lift history (strouhal_analyzer.cpp:39-84:
  * mean removed, Hann window over the first min(n, 4096) samples, radix-2 FFT,
  * peak bin >= 1). Returns the frequency; St = f D / U. */

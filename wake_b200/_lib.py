@@ -108,6 +108,23 @@ _PROTOS = {
     "wake_grid_launches_per_step": (I, [vp]),
     "wake_grid_time_bulk_launches": (I, [vp, I]),
     "wake_grid_bulk_launch_times": (I, [vp, vp, vp, vp]),
+    "wake_grid_set_solid_ellipse": (I, [vp, F, F, F, F, F]),
+    "wake_grid_device_bytes": (LL, [vp]),
+    "wake_grid_estimate_bytes": (LL, [I, I, I, I, I, I]),
+    "wake_grid_release_scratch": (I, [vp]),
+    "wake_batch_create": (vp, [I, I]),
+    "wake_batch_destroy": (None, [vp]),
+    "wake_batch_add": (I, [vp, vp]),
+    "wake_batch_remove": (I, [vp, vp]),
+    "wake_batch_size": (I, [vp]),
+    "wake_batch_set_stream": (I, [vp, vp]),
+    "wake_batch_use_graph": (I, [vp, I]),
+    "wake_batch_set_block": (I, [vp, I, I]),
+    "wake_batch_get_block": (I, [vp]),
+    "wake_batch_step": (I, [vp, I]),
+    "wake_batch_synchronize": (I, [vp]),
+    "wake_batch_info": (I, [vp, vp, vp, vp, vp]),
+    "wake_batch_autotune": (I, [vp, I, vp]),
     "wake_strouhal_frequency": (D, [vp, I, D]),
 }
 

@@ -13,9 +13,7 @@
 #include <string>
 #include <vector>
 
-#include "common.cuh"
-#include "kernels.cuh"
-#include "wake_gpu.h"
+#include "engine.cuh"
 
 namespace wk {
 
@@ -34,33 +32,16 @@ void clear_error() {
     t_code = 0;
 }
 
-// ---------------------------------------------------------------- host lattice tables
-struct HostLat {
-    int Q = 0, D = 0;
-    int cx[27], cy[27], cz[27], opp[27];
-    float w[27];
-    explicit HostLat(int q) : Q(q) {
-        auto fill = [&](auto lat) {
-            using L = decltype(lat);
-            D = L::D;
-            for (int k = 0; k < Q; ++k) {
-                cx[k] = L::cx(k);
-                cy[k] = L::cy(k);
-                cz[k] = L::cz(k);
-                opp[k] = L::opp(k);
-                w[k] = L::w(k);
-            }
-        };
-        if (q == 9) fill(Lat<9>{});
-        else if (q == 19) fill(Lat<19>{});
-        else fill(Lat<27>{});
-    }
-};
-
 cudaError_t launch_step_any(int Q, int coll, int store, bool les, const StepArgs& a, const Launch& L, bool fast) {
     if (Q == 9) return launch_step_q9(coll, store, les, a, L, fast);
     if (Q == 19) return launch_step_q19(coll, store, les, a, L, fast);
     return launch_step_q27(coll, store, les, a, L, fast);
+}
+cudaError_t launch_batch_any(int Q, int coll, int store, bool les, const BatchArgs& b, int tpb, cudaStream_t stream,
+                             bool fast, bool idx32) {
+    if (Q == 9) return launch_batch_q9(coll, store, les, b, tpb, stream, fast, idx32);
+    if (Q == 19) return launch_batch_q19(coll, store, les, b, tpb, stream, fast, idx32);
+    return launch_batch_q27(coll, store, les, b, tpb, stream, fast, idx32);
 }
 cudaError_t launch_initial_any(int Q, int coll, int store, bool les, const float* f0, void* a, void* b,
                                const uint8_t* flags, const Geo& geo, const Physics& phys, const Launch& L) {
@@ -140,25 +121,7 @@ __global__ void k_diag_partials(const float* __restrict__ rho, const float* __re
 // wrote the slots, on the same stream.
 __global__ void __launch_bounds__(256) k_mem_reduce(const double* __restrict__ contrib, int n, unsigned* hist_step,
                                                     double* hist, int hist_cap) {
-    __shared__ double red[3][256];
-    double s[3] = {0.0, 0.0, 0.0};
-    for (int j = threadIdx.x; j < n; j += 256)
-        for (int c = 0; c < 3; ++c) s[c] += contrib[3 * static_cast<long long>(j) + c];
-    for (int c = 0; c < 3; ++c) red[c][threadIdx.x] = s[c];
-    __syncthreads();
-    for (int o = 128; o > 0; o >>= 1) {
-        if (threadIdx.x < o)
-            for (int c = 0; c < 3; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + o];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        const unsigned step = *hist_step;
-        double* h = hist + 3 * static_cast<long long>(step % static_cast<unsigned>(hist_cap));
-        h[0] = red[0][0];
-        h[1] = red[1][0];
-        h[2] = red[2][0];
-        *hist_step = step + 1u;
-    }
+    mem_reduce_block(contrib, n, hist_step, hist, hist_cap);
 }
 
 cudaError_t launch_link_marks(const int* link_node, int n_links, uint8_t* flags, int* node_start,
@@ -173,148 +136,6 @@ cudaError_t launch_link_marks(const int* link_node, int n_links, uint8_t* flags,
 using namespace wk;
 
 // ==================================================================== grid
-struct wake_grid {
-    int Q = 0, D = 0, nx = 0, ny = 0, nz = 0, storage = 0;
-    long long N = 0, pitch = 0;
-    std::size_t elem = 4;
-    HostLat lat{9};
-
-    DevMem A, B;       // state buffers
-    int cur = 0;       // 0: A holds the current state, 1: B
-    // State machine. m_f (FP32) holds the reference-visible f^k whenever mf_valid.
-    // `pending`: A/B do not hold Collide(f^k) for the current collision parameters
-    // (fresh initial state, or tau / model / body force changed since the last
-    // collide); the next step re-collides f^k from m_f first, exactly like the
-    // reference, whose step k+1 starts by colliding f^k with that step's parameters.
-    bool pending = true;
-    bool mf_valid = false;
-    float collided_g[3] = {0.f, 0.f, 0.f};  // body force the state buffers were collided with
-    float last_step_g[3] = {0.f, 0.f, 0.f};  // body force of the last executed step
-    DevMem d_types, d_flags, d_status, d_nodestart;
-    std::vector<uint8_t> types;
-    bool geom_dirty = true;
-
-    int collision = WAKE_MRT, les = 0;
-    Physics phys{};
-    int inflow = 0, outflow = 0, lid = 0, periodic_y = 0, periodic_z = 0;
-    float uin[3] = {0.f, 0.f, 0.f}, rho_out = 1.0f, uw[3] = {0.f, 0.f, 0.f};
-
-    std::vector<int> link_node, link_q;
-    std::vector<float> link_delta, link_uw;  // uw: 3 per link
-    DevMem d_link_node, d_link_q, d_link_delta, d_link_mom;
-    int dev_links = 0;         // links currently on the device (the flags refer to these)
-    bool links_dirty = false;  // host links differ from the device copy
-
-    int mem_on = 0, hist_cap = 0;
-    float center[3] = {0.f, 0.f, 0.f}, rmax = 0.f;
-    DevMem d_counters, d_hist;         // counters: [0] unused, [1] history entries written
-    DevMem d_warp_base, d_contrib;     // momentum-exchange slots (see MemCfg)
-    int warps_per_row = 1, n_mem_nodes = 0;
-
-    // rows handled by k_step_fast (pure-gather rows) and by k_step (the rest),
-    // packed (z << 16) | y
-    DevMem d_fast_rows, d_gen_rows;
-    int n_fast = 0, n_gen = 0;
-
-    int tpb = 0, xchunks = 1, rows = 1, tpb_fast = 256;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    cudaStream_t side = nullptr;  // forked stream of the general-row launch
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    long long k = 0;
-
-    DevMem m_f, m_rho, m_ux, m_uy, m_uz, m_speed, m_diag;
-
-    // CUDA graph of `graph_steps` fused steps starting from buffer parity graph_cur
-    cudaGraphExec_t graph = nullptr;
-    int graph_steps = 0, graph_cur = -1;
-    float graph_g[3] = {0.f, 0.f, 0.f};
-    bool graph_ok = false;
-
-    // Optional CUDA-event timing of every pure-gather (bulk) launch; plain launches only.
-    bool time_bulk = false;
-    std::vector<cudaEvent_t> t_ev;  // pairs (start, end), reused
-    std::size_t t_used = 0;         // events recorded since the last read
-
-    explicit wake_grid(int q) : lat(q) {}
-    ~wake_grid() {
-        for (cudaEvent_t e : t_ev) cudaEventDestroy(e);
-        if (graph) cudaGraphExecDestroy(graph);
-        if (own_stream && stream) cudaStreamDestroy(stream);
-        if (side) cudaStreamDestroy(side);
-        if (ev_fork) cudaEventDestroy(ev_fork);
-        if (ev_join) cudaEventDestroy(ev_join);
-    }
-
-    void* buf(int which) { return which == 0 ? A.p : B.p; }
-
-    Geo geo() const {
-        Geo g{};
-        g.nx = nx;
-        g.ny = ny;
-        g.nz = nz;
-        g.periodic_y = (D == 3) ? periodic_y : 0;
-        g.periodic_z = (D == 3) ? periodic_z : 0;
-        g.pitch = pitch;
-        for (int a = 0; a < 3; ++a) g.uin[a] = uin[a];
-        g.rho_out = rho_out;
-        for (int q = 0; q < Q; ++q) {
-            // 2 w_q rho_0 / cs^2 (c_q . u_w) in the reference's float order (d2q9_streaming.ispc:49-53)
-            const float ci_uw = float(lat.cx[q]) * uw[0] + float(lat.cy[q]) * uw[1] + float(lat.cz[q]) * uw[2];
-            g.mom[q] = lid ? 2.0f * lat.w[q] * 1.0f * 3.0f * ci_uw : 0.0f;
-        }
-        return g;
-    }
-    Links links() const {
-        Links l{};
-        l.node_start = d_nodestart.as<int>();
-        l.node = d_link_node.as<int>();
-        l.q = d_link_q.as<int>();
-        l.delta = d_link_delta.as<float>();
-        l.mom = d_link_mom.as<float>();
-        l.count = dev_links;
-        return l;
-    }
-    Launch launch() const { return Launch{tpb, xchunks, rows, stream, ny, nz, tpb_fast}; }
-    int blocks() const { return rows * xchunks; }
-
-    void invalidate_graph() { graph_ok = false; }
-
-    void choose_block(int want) {
-        const int full = ((nx + 31) / 32) * 32;
-        if (want > 0) tpb = want;
-        else if (full <= 512) tpb = full;
-        else {
-            int best = 256;
-            long long best_waste = -1;
-            for (int t : {256, 384, 512}) {
-                const long long chunks = (nx + t - 1) / t;
-                const long long waste = chunks * t - nx;
-                if (best_waste < 0 || waste < best_waste) {
-                    best = t;
-                    best_waste = waste;
-                }
-            }
-            tpb = best;
-        }
-        xchunks = (nx + tpb - 1) / tpb;
-        rows = ny * nz;
-        // k_step_fast is limited to 256 threads (four blocks per SM). Least idle lanes over the row,
-        // ties to the smaller block: 64-thread blocks measured fastest on 256-node rows (more
-        // independent blocks in flight per SM, shorter tail per row).
-        const int cap = std::min(want > 0 ? want : 256, 256);
-        int best = -1, best_waste = 1 << 30;
-        for (int t = 64; t <= cap; t += 32) {
-            const int waste = ((nx + t - 1) / t) * t - nx;
-            if (waste < best_waste) {
-                best = t;
-                best_waste = waste;
-            }
-        }
-        tpb_fast = best > 0 ? best : 64;
-    }
-};
-
 namespace {
 
 bool valid_grid(wake_grid* g) {
@@ -411,7 +232,10 @@ int rebuild_flags(wake_grid* g) {
             WK_CUDA(g->d_contrib.ensure(sizeof(double) * 3 * std::max(1, count)));
         }
         WK_CUDA(cudaStreamSynchronize(g->stream));  // the host vectors go out of scope
+        g->h_fast_rows = std::move(fast);
+        g->h_gen_rows = std::move(gen);
     }
+    ++g->geom_version;
     g->geom_dirty = false;
     g->invalidate_graph();
     return WAKE_OK;
@@ -570,27 +394,9 @@ void equilibrium(const HostLat& lat, float rho, float ux, float uy, float uz, fl
 
 int do_steps(wake_grid* g, int n) {
     for (int s = 0; s < n; ++s) {
-        StepArgs a{};
+        StepArgs a = wk::grid_step_args(g);
         a.fin = g->buf(g->cur);
         a.fout = g->buf(1 - g->cur);
-        a.flags = g->d_flags.as<uint8_t>();
-        a.status = g->d_status.as<unsigned>();
-        a.geo = g->geo();
-        a.links = g->links();
-        a.mem.enabled = g->mem_on;
-        if (g->mem_on) {
-            for (int c = 0; c < 3; ++c) a.mem.center[c] = g->center[c];
-            a.mem.r_max = g->rmax;
-            a.mem.r_max_sq = g->rmax * g->rmax;
-            a.mem.warp_base = g->d_warp_base.as<int>();
-            a.mem.warps_per_row = g->warps_per_row;
-            a.mem.contrib = g->d_contrib.as<double>();
-            a.mem.n_nodes = g->n_mem_nodes;
-            a.mem.hist_step = g->d_counters.as<unsigned>() + 1;
-            a.mem.hist = g->d_hist.as<double>();
-            a.mem.hist_cap = g->hist_cap;
-        }
-        a.phys = g->phys;
         // The pure-gather rows and the rows with boundaries / momentum exchange write
         // disjoint nodes of the output, so the small general launch runs on a forked
         // stream beside the bulk launch (a fork/join that CUDA graph capture keeps).
@@ -640,6 +446,46 @@ int do_steps(wake_grid* g, int n) {
 }
 
 }  // namespace
+
+namespace wk {
+
+bool grid_valid(wake_grid* g) { return valid_grid(g); }
+int grid_prepare(wake_grid* g) { return prepare(g); }
+
+StepArgs grid_step_args(const wake_grid* g) {
+    StepArgs a{};
+    a.flags = g->d_flags.as<uint8_t>();
+    a.status = g->d_status.as<unsigned>();
+    a.geo = g->geo();
+    a.links = g->links();
+    a.mem.enabled = g->mem_on;
+    if (g->mem_on) {
+        for (int c = 0; c < 3; ++c) a.mem.center[c] = g->center[c];
+        a.mem.r_max = g->rmax;
+        a.mem.r_max_sq = g->rmax * g->rmax;
+        a.mem.warp_base = g->d_warp_base.as<int>();
+        a.mem.warps_per_row = g->warps_per_row;
+        a.mem.contrib = g->d_contrib.as<double>();
+        a.mem.n_nodes = g->n_mem_nodes;
+        a.mem.hist_step = g->d_counters.as<unsigned>() + 1;
+        a.mem.hist = g->d_hist.as<double>();
+        a.mem.hist_cap = g->hist_cap;
+    }
+    a.phys = g->phys;
+    return a;
+}
+
+void grid_advanced(wake_grid* g, int n) {
+    if (n <= 0) return;
+    g->cur ^= (n & 1);
+    g->k += n;
+    g->mf_valid = false;
+    for (int c = 0; c < 3; ++c) g->last_step_g[c] = g->phys.g[c];
+}
+
+int grid_check_status(wake_grid* g) { return wake_grid_synchronize(g); }
+
+}  // namespace wk
 
 // ==================================================================== C ABI
 extern "C" {
@@ -818,6 +664,32 @@ int wake_grid_set_solid_sphere(wake_grid* g, float cx, float cy, float cz, float
                 const float dx = static_cast<float>(x) - cx, dy = static_cast<float>(y) - cy,
                             dz = static_cast<float>(z) - cz;
                 if (dx * dx + dy * dy + dz * dz <= r_sq) g->types[idx3(g, x, y, z)] = WAKE_CELL_SOLID;
+            }
+    g->geom_dirty = true;
+    return WAKE_OK;
+}
+
+// Rotated ellipse (no reference counterpart; same cell-centre rule and float
+// arithmetic as GeometryPrimitives::voxelize_ellipsoid, src/geometry/primitives.cpp:73-99):
+// node (x, y) is solid when u^2/a^2 + v^2/b^2 <= 1 with (u, v) the offset from
+// (cx, cy) rotated by -angle (radians), u = dx cos + dy sin, v = -dx sin + dy cos.
+// Extruded along z in 3D.
+int wake_grid_set_solid_ellipse(wake_grid* g, float cx, float cy, float a, float b, float angle) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (!(a > 0.f) || !(b > 0.f)) return set_error(WAKE_ERR_INVALID, "wake_grid_set_solid_ellipse: semi-axes must be positive");
+    const float r = std::max(a, b);
+    const int min_x = std::max(0, static_cast<int>(cx - r - 1));
+    const int max_x = std::min(g->nx - 1, static_cast<int>(cx + r + 1));
+    const int min_y = std::max(0, static_cast<int>(cy - r - 1));
+    const int max_y = std::min(g->ny - 1, static_cast<int>(cy + r + 1));
+    const float c = std::cos(angle), s = std::sin(angle);
+    const float inv_a2 = 1.0f / (a * a), inv_b2 = 1.0f / (b * b);
+    for (int z = 0; z < g->nz; ++z)
+        for (int y = min_y; y <= max_y; ++y)
+            for (int x = min_x; x <= max_x; ++x) {
+                const float dx = static_cast<float>(x) - cx, dy = static_cast<float>(y) - cy;
+                const float u = dx * c + dy * s, v = -dx * s + dy * c;
+                if (u * u * inv_a2 + v * v * inv_b2 <= 1.0f) g->types[idx3(g, x, y, z)] = WAKE_CELL_SOLID;
             }
     g->geom_dirty = true;
     return WAKE_OK;
@@ -1177,6 +1049,46 @@ int wake_grid_info(wake_grid* g, int* q, int* nx, int* ny, int* nz, int* storage
     if (nz) *nz = g->nz;
     if (storage) *storage = g->storage;
     if (pitch) *pitch = g->pitch;
+    return WAKE_OK;
+}
+
+long long wake_grid_device_bytes(wake_grid* g) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    const DevMem* all[] = {&g->A, &g->B, &g->d_types, &g->d_flags, &g->d_status, &g->d_nodestart, &g->d_link_node,
+                           &g->d_link_q, &g->d_link_delta, &g->d_link_mom, &g->d_counters, &g->d_hist,
+                           &g->d_warp_base, &g->d_contrib, &g->d_fast_rows, &g->d_gen_rows, &g->m_f, &g->m_rho,
+                           &g->m_ux, &g->m_uy, &g->m_uz, &g->m_speed, &g->m_diag};
+    long long sum = 0;
+    for (const DevMem* m : all) sum += static_cast<long long>(m->bytes);
+    return sum;
+}
+
+long long wake_grid_estimate_bytes(int q, int nx, int ny, int nz, int storage, int with_fields) {
+    if (!(q == 9 || q == 19 || q == 27) || nx < 1 || ny < 1 || nz < 1 || storage < 0 || storage > 2)
+        return set_error(WAKE_ERR_INVALID, "wake_grid_estimate_bytes: invalid lattice, size or storage");
+    const long long N = static_cast<long long>(nx) * ny * nz, pitch = (N + 63) / 64 * 64;
+    const long long elem = storage == WAKE_STORE_F32 ? 4 : 2;
+    long long b = 2 * q * pitch * elem;  // state buffers
+    b += q * pitch * 4;                  // FP32 populations for (re)initialisation
+    b += 2 * N + 4 * N;                  // cell types, flags, per-node first curved link
+    b += 8ll * ny * nz;                  // row lists
+    if (with_fields) b += 5 * 4 * N;     // rho, ux, uy, uz, speed
+    return b + (1ll << 20);              // history ring, slots and small tables
+}
+
+int wake_grid_release_scratch(wake_grid* g) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    const int r = prepare(g);  // a pending re-collide consumes the FP32 populations first
+    if (r) return r;
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    g->m_f.reset();
+    g->mf_valid = false;
+    g->m_rho.reset();
+    g->m_ux.reset();
+    g->m_uy.reset();
+    g->m_uz.reset();
+    g->m_speed.reset();
+    g->m_diag.reset();
     return WAKE_OK;
 }
 

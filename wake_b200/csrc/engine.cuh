@@ -1,0 +1,210 @@
+// Host state of one resident lattice (wake_grid) shared by the single-lattice
+// engine (engine.cu) and the batch of many lattices (batch.cu).
+#pragma once
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "wake_gpu.h"
+
+namespace wk {
+
+// ---------------------------------------------------------------- host lattice tables
+struct HostLat {
+    int Q = 0, D = 0;
+    int cx[27], cy[27], cz[27], opp[27];
+    float w[27];
+    explicit HostLat(int q) : Q(q) {
+        auto fill = [&](auto lat) {
+            using L = decltype(lat);
+            D = L::D;
+            for (int k = 0; k < Q; ++k) {
+                cx[k] = L::cx(k);
+                cy[k] = L::cy(k);
+                cz[k] = L::cz(k);
+                opp[k] = L::opp(k);
+                w[k] = L::w(k);
+            }
+        };
+        if (q == 9) fill(Lat<9>{});
+        else if (q == 19) fill(Lat<19>{});
+        else fill(Lat<27>{});
+    }
+};
+
+cudaError_t launch_step_any(int Q, int coll, int store, bool les, const StepArgs& a, const Launch& L, bool fast);
+cudaError_t launch_batch_any(int Q, int coll, int store, bool les, const BatchArgs& b, int tpb, cudaStream_t stream,
+                             bool fast, bool idx32);
+
+}  // namespace wk
+
+using wk::DevMem;
+using wk::HostLat;
+using wk::Physics;
+using wk::Geo;
+using wk::Links;
+using wk::Launch;
+using wk::StepArgs;
+
+struct wake_grid {
+    int Q = 0, D = 0, nx = 0, ny = 0, nz = 0, storage = 0;
+    long long N = 0, pitch = 0;
+    std::size_t elem = 4;
+    HostLat lat{9};
+
+    DevMem A, B;       // state buffers
+    int cur = 0;       // 0: A holds the current state, 1: B
+    // State machine. m_f (FP32) holds the reference-visible f^k whenever mf_valid.
+    // `pending`: A/B do not hold Collide(f^k) for the current collision parameters
+    // (fresh initial state, or tau / model / body force changed since the last
+    // collide); the next step re-collides f^k from m_f first, exactly like the
+    // reference, whose step k+1 starts by colliding f^k with that step's parameters.
+    bool pending = true;
+    bool mf_valid = false;
+    float collided_g[3] = {0.f, 0.f, 0.f};  // body force the state buffers were collided with
+    float last_step_g[3] = {0.f, 0.f, 0.f};  // body force of the last executed step
+    DevMem d_types, d_flags, d_status, d_nodestart;
+    std::vector<uint8_t> types;
+    bool geom_dirty = true;
+
+    int collision = WAKE_MRT, les = 0;
+    Physics phys{};
+    int inflow = 0, outflow = 0, lid = 0, periodic_y = 0, periodic_z = 0;
+    float uin[3] = {0.f, 0.f, 0.f}, rho_out = 1.0f, uw[3] = {0.f, 0.f, 0.f};
+
+    std::vector<int> link_node, link_q;
+    std::vector<float> link_delta, link_uw;  // uw: 3 per link
+    DevMem d_link_node, d_link_q, d_link_delta, d_link_mom;
+    int dev_links = 0;         // links currently on the device (the flags refer to these)
+    bool links_dirty = false;  // host links differ from the device copy
+
+    int mem_on = 0, hist_cap = 0;
+    float center[3] = {0.f, 0.f, 0.f}, rmax = 0.f;
+    DevMem d_counters, d_hist;         // counters: [0] unused, [1] history entries written
+    DevMem d_warp_base, d_contrib;     // momentum-exchange slots (see MemCfg)
+    int warps_per_row = 1, n_mem_nodes = 0;
+
+    // rows handled by k_step_fast (pure-gather rows) and by k_step (the rest),
+    // packed (z << 16) | y
+    DevMem d_fast_rows, d_gen_rows;
+    int n_fast = 0, n_gen = 0;
+    std::vector<unsigned> h_fast_rows, h_gen_rows;  // host copies of the two row lists
+    unsigned geom_version = 0;                      // bumped whenever the flags / row lists are rebuilt
+
+    int tpb = 0, xchunks = 1, rows = 1, tpb_fast = 256;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaStream_t side = nullptr;  // forked stream of the general-row launch
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    long long k = 0;
+
+    DevMem m_f, m_rho, m_ux, m_uy, m_uz, m_speed, m_diag;
+
+    // CUDA graph of `graph_steps` fused steps starting from buffer parity graph_cur
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0, graph_cur = -1;
+    float graph_g[3] = {0.f, 0.f, 0.f};
+    bool graph_ok = false;
+
+    // Optional CUDA-event timing of every pure-gather (bulk) launch; plain launches only.
+    bool time_bulk = false;
+    std::vector<cudaEvent_t> t_ev;  // pairs (start, end), reused
+    std::size_t t_used = 0;         // events recorded since the last read
+
+    explicit wake_grid(int q) : lat(q) {}
+    ~wake_grid() {
+        for (cudaEvent_t e : t_ev) cudaEventDestroy(e);
+        if (graph) cudaGraphExecDestroy(graph);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+        if (side) cudaStreamDestroy(side);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+    }
+
+    void* buf(int which) { return which == 0 ? A.p : B.p; }
+
+    Geo geo() const {
+        Geo g{};
+        g.nx = nx;
+        g.ny = ny;
+        g.nz = nz;
+        g.periodic_y = (D == 3) ? periodic_y : 0;
+        g.periodic_z = (D == 3) ? periodic_z : 0;
+        g.pitch = pitch;
+        for (int a = 0; a < 3; ++a) g.uin[a] = uin[a];
+        g.rho_out = rho_out;
+        for (int q = 0; q < Q; ++q) {
+            // 2 w_q rho_0 / cs^2 (c_q . u_w) in the reference's float order (d2q9_streaming.ispc:49-53)
+            const float ci_uw = float(lat.cx[q]) * uw[0] + float(lat.cy[q]) * uw[1] + float(lat.cz[q]) * uw[2];
+            g.mom[q] = lid ? 2.0f * lat.w[q] * 1.0f * 3.0f * ci_uw : 0.0f;
+        }
+        return g;
+    }
+    Links links() const {
+        Links l{};
+        l.node_start = d_nodestart.as<int>();
+        l.node = d_link_node.as<int>();
+        l.q = d_link_q.as<int>();
+        l.delta = d_link_delta.as<float>();
+        l.mom = d_link_mom.as<float>();
+        l.count = dev_links;
+        return l;
+    }
+    Launch launch() const { return Launch{tpb, xchunks, rows, stream, ny, nz, tpb_fast}; }
+    int blocks() const { return rows * xchunks; }
+
+    void invalidate_graph() { graph_ok = false; }
+
+    void choose_block(int want) {
+        const int full = ((nx + 31) / 32) * 32;
+        if (want > 0) tpb = want;
+        else if (full <= 512) tpb = full;
+        else {
+            int best = 256;
+            long long best_waste = -1;
+            for (int t : {256, 384, 512}) {
+                const long long chunks = (nx + t - 1) / t;
+                const long long waste = chunks * t - nx;
+                if (best_waste < 0 || waste < best_waste) {
+                    best = t;
+                    best_waste = waste;
+                }
+            }
+            tpb = best;
+        }
+        xchunks = (nx + tpb - 1) / tpb;
+        rows = ny * nz;
+        // k_step_fast is limited to 256 threads (four blocks per SM). Least idle lanes over the row,
+        // ties to the smaller block: 64-thread blocks measured fastest on 256-node rows (more
+        // independent blocks in flight per SM, shorter tail per row).
+        const int cap = std::min(want > 0 ? want : 256, 256);
+        int best = -1, best_waste = 1 << 30;
+        for (int t = 64; t <= cap; t += 32) {
+            const int waste = ((nx + t - 1) / t) * t - nx;
+            if (waste < best_waste) {
+                best = t;
+                best_waste = waste;
+            }
+        }
+        tpb_fast = best > 0 ? best : 64;
+    }
+};
+
+namespace wk {
+
+// Validity check that records the error (WAKE_ERR_INVALID) for a null handle.
+bool grid_valid(wake_grid* g);
+// Bring a lattice to the point where its state buffers hold Collide(f^k) for the
+// current geometry and parameters (rebuilds flags, re-collides when pending).
+int grid_prepare(wake_grid* g);
+// Step arguments of one lattice (rows and buffers left for the caller).
+StepArgs grid_step_args(const wake_grid* g);
+// Bookkeeping after n steps run outside wake_grid_step (by a batch).
+void grid_advanced(wake_grid* g, int n);
+// Error status word of the lattice: WAKE_OK or WAKE_ERR_NUMERIC (synchronizes its stream).
+int grid_check_status(wake_grid* g);
+
+}  // namespace wk

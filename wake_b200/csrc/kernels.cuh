@@ -28,6 +28,8 @@ struct FlagCfg {
 // Per-lattice entry points (defined once per Q in kernels_impl.cuh).
 #define WK_DECLARE_LAUNCHERS(Q)                                                                                   \
     cudaError_t launch_step_q##Q(int coll, int store, bool les, const StepArgs& a, const Launch& L, bool fast);  \
+    cudaError_t launch_batch_q##Q(int coll, int store, bool les, const BatchArgs& b, int tpb,                   \
+                                  cudaStream_t stream, bool fast, bool idx32);                                  \
     cudaError_t launch_materialise_q##Q(int store, const void* fin, const uint8_t* flags, const Geo& geo,        \
                                         const Links& links, const Physics& phys, const Out& out,                 \
                                         const Launch& L, int direct);                                            \

@@ -142,7 +142,18 @@ void initial_one(const float* f0, void* A, void* B, const uint8_t* flags, const 
                  const Launch& L) {
     k_initial<kQ, C, S, LES><<<L.rows * L.xchunks, L.tpb, 0, L.stream>>>(f0, A, B, flags, g, p, L.xchunks);
 }
+template <int C, int S, bool LES>
+void batch_one(const BatchArgs& b, int tpb, cudaStream_t st, bool fast, bool idx32) {
+    if (b.nrows <= 0) return;
+    if (fast) {
+        if (idx32) k_step_fast_batch<kQ, C, S, LES, true><<<b.nrows, tpb, 0, st>>>(b);
+        else k_step_fast_batch<kQ, C, S, LES, false><<<b.nrows, tpb, 0, st>>>(b);
+    } else {
+        k_step_batch<kQ, C, S, LES><<<b.nrows, tpb, 0, st>>>(b);
+    }
+}
 using StepFn = void (*)(const StepArgs&, const Launch&, bool);
+using BatchFn = void (*)(const BatchArgs&, int, cudaStream_t, bool, bool);
 using InitFn = void (*)(const float*, void*, void*, const uint8_t*, const Geo&, const Physics&, const Launch&);
 
 #define WK_ROW(C, S) {step_one<C, S, false>, step_one<C, S, true>}
@@ -153,8 +164,13 @@ const StepFn kStep[3][3][2] = {{WK_ROW(0, 0), WK_ROW(0, 1), WK_ROW(0, 2)},
 const InitFn kInit[3][3][2] = {{WK_IROW(0, 0), WK_IROW(0, 1), WK_IROW(0, 2)},
                                {WK_IROW(1, 0), WK_IROW(1, 1), WK_IROW(1, 2)},
                                {WK_IROW(2, 0), WK_IROW(2, 1), WK_IROW(2, 2)}};
+#define WK_BROW(C, S) {batch_one<C, S, false>, batch_one<C, S, true>}
+const BatchFn kBatch[3][3][2] = {{WK_BROW(0, 0), WK_BROW(0, 1), WK_BROW(0, 2)},
+                                 {WK_BROW(1, 0), WK_BROW(1, 1), WK_BROW(1, 2)},
+                                 {WK_BROW(2, 0), WK_BROW(2, 1), WK_BROW(2, 2)}};
 #undef WK_ROW
 #undef WK_IROW
+#undef WK_BROW
 
 bool valid(int coll, int store) { return coll >= 0 && coll < 3 && store >= 0 && store < 3; }
 }  // namespace
@@ -163,6 +179,13 @@ cudaError_t WK_CAT(launch_step_q, WK_Q)(int coll, int store, bool les, const Ste
                                        bool fast) {
     if (!valid(coll, store)) return cudaErrorInvalidValue;
     kStep[coll][store][les ? 1 : 0](a, L, fast);
+    return cudaGetLastError();
+}
+
+cudaError_t WK_CAT(launch_batch_q, WK_Q)(int coll, int store, bool les, const BatchArgs& b, int tpb,
+                                        cudaStream_t stream, bool fast, bool idx32) {
+    if (!valid(coll, store)) return cudaErrorInvalidValue;
+    kBatch[coll][store][les ? 1 : 0](b, tpb, stream, fast, idx32);
     return cudaGetLastError();
 }
 

@@ -215,6 +215,25 @@ __device__ __forceinline__ float sqrt_approx(float x) {
     return r;
 }
 
+// tau_eff = (tau0 + sqrt(tau0^2 + 18 sqrt(2) Cs^2 sqrt(2 Pi:Pi) / rho)) / 2
+// (d3q19_les.ispc:49-55 form). The approximate square root and division (a few
+// ulp) cost a fraction of the exact sequences and perturb tau by ~1e-7. Every
+// rounding is explicit, so the bits do not depend on which products of the
+// loop-invariant tau0 / Cs the compiler hoists out of a kernel's node loop: a
+// lattice gets the same tau_eff from every kernel that inlines this.
+__device__ __forceinline__ float smagorinsky_tau_eff(float tau0, float cs, float rho, float sum) {
+    const float qs = sqrt_approx(__fmul_rn(2.0f, sum));
+    const float pref = __fmul_rn(__fmul_rn(18.0f * 1.4142135623730951f, cs), cs);
+    const float t2 = __fmul_rn(tau0, tau0);
+    return __fmul_rn(0.5f, __fadd_rn(tau0, sqrt_approx(__fmaf_rn(__fdividef(pref, rho), qs, t2))));
+}
+
+// TRT antisymmetric rate for a per-node tau (Lambda = (tau_s - 1/2)(tau_a - 1/2)),
+// rounding explicit for the same reason.
+__device__ __forceinline__ float trt_tau_a(float lambda, float tau) {
+    return __fadd_rn(0.5f, __fdividef(lambda, fmaxf(1e-4f, __fsub_rn(tau, 0.5f))));
+}
+
 // Because c_opp = -c, the second-order tensor only sees the even part of each
 // (q, opp) pair: Pi = sum over pairs c c^T (f_q + f_opp - 2 w rho (1 + 4.5 (c.u)^2 - 1.5 u^2)).
 // The same even parts feed the TRT update, so the compiler shares them.
@@ -239,11 +258,7 @@ __device__ __forceinline__ float smagorinsky_tau(const float* f, float rho, cons
         if (x && z) pxz += (x * z > 0) ? fn : -fn;
     }
     const float sum = pxx * pxx + pyy * pyy + pzz * pzz + 2.0f * (pxy * pxy + pyz * pyz + pxz * pxz);
-    // per-node relaxation time: the approximate square root and division (a few
-    // ulp) cost a fraction of the exact sequences and perturb tau by ~1e-7
-    const float qs = sqrt_approx(2.0f * sum);
-    const float pref = 18.0f * 1.4142135623730951f * cs * cs;
-    return 0.5f * (tau0 + sqrt_approx(tau0 * tau0 + __fdividef(pref, rho) * qs));
+    return smagorinsky_tau_eff(tau0, cs, rho, sum);
 }
 
 template <int Q>
@@ -356,11 +371,9 @@ __device__ __forceinline__ void trt_pairs(float* f, const Physics& P, float& rho
             if (x && z) pxz += (x * z > 0) ? fn : -fn;
         }
         const float sum = pxx * pxx + pyy * pyy + pzz * pzz + 2.0f * (pxy * pxy + pyz * pyz + pxz * pxz);
-        const float pref = 18.0f * 1.4142135623730951f * P.cs_smag * P.cs_smag;
-        const float tau = 0.5f * (P.tau + sqrt_approx(P.tau * P.tau + __fdividef(pref, r) * sqrt_approx(2.0f * sum)));
-        const float tau_a = 0.5f + __fdividef(P.lambda_trt, fmaxf(1e-4f, tau - 0.5f));
+        const float tau = smagorinsky_tau_eff(P.tau, P.cs_smag, r, sum);
         os = __fdividef(1.0f, tau);
-        oa = __fdividef(1.0f, tau_a);
+        oa = __fdividef(1.0f, trt_tau_a(P.lambda_trt, tau));
     } else {
         const float tau_a = 0.5f + P.lambda_trt / fmaxf(1e-4f, P.tau - 0.5f);
         os = 1.0f / P.tau;
@@ -720,8 +733,7 @@ __device__ __forceinline__ void collide(float* f, float rho, const float u[3], c
         // tau_a from the magic parameter (lattice_grid_2d.cpp:219-222)
         if (LES) {
             // per-node rates: approximate divisions (see smagorinsky_tau)
-            const float tau_a = 0.5f + __fdividef(P.lambda_trt, fmaxf(1e-4f, tau - 0.5f));
-            collide_trt_omega<Q>(f, rho, u, P.g, __fdividef(1.0f, tau), __fdividef(1.0f, tau_a));
+            collide_trt_omega<Q>(f, rho, u, P.g, __fdividef(1.0f, tau), __fdividef(1.0f, trt_tau_a(P.lambda_trt, tau)));
         } else {
             const float tau_a = 0.5f + P.lambda_trt / fmaxf(1e-4f, tau - 0.5f);
             collide_trt<Q>(f, rho, u, P.g, tau, tau_a);

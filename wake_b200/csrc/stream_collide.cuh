@@ -220,15 +220,15 @@ struct StepArgs {
     int nrows;
 };
 
-// One fused time step: g^{k+1} = Collide(ZouHe(BFL(Pull(g^k)))). Solid nodes are not
-// touched: both buffers hold their frozen populations.
+// One fused time step of one row: g^{k+1} = Collide(ZouHe(BFL(Pull(g^k)))). Solid
+// nodes are not touched: both buffers hold their frozen populations. `e` is the row
+// (z << 16) | y, `entry` its index in the launch's general-row list (momentum-exchange
+// slots are numbered per entry).
 template <int Q, int COLL, int S, bool LES>
-__global__ void __launch_bounds__(512) k_step(const StepArgs a) {
+__device__ __forceinline__ void step_row(const StepArgs& a, unsigned e, int entry) {
     using L = Lat<Q>;
     using C = Codec<S>;
     using T = typename C::T;
-    // one block per listed row; the threads stride along x
-    const unsigned e = a.rows[blockIdx.x];
     const int y = static_cast<int>(e & 0xffffu), z = static_cast<int>(e >> 16);
     const long long row0 = (static_cast<long long>(z) * a.geo.ny + y) * a.geo.nx;
     const int nx = a.geo.nx, lane = threadIdx.x & 31;
@@ -244,8 +244,7 @@ __global__ void __launch_bounds__(512) k_step(const StepArgs a) {
             const unsigned live = (nx - xb >= 32) ? 0xffffffffu : ((1u << (nx - xb)) - 1u);
             const bool m = (fl & FL_MEM) != 0;
             const unsigned bal = __ballot_sync(live, m);
-            if (m) slot = a.mem.warp_base[blockIdx.x * a.mem.warps_per_row + (xb >> 5)] +
-                          __popc(bal & ((1u << lane) - 1u));
+            if (m) slot = a.mem.warp_base[entry * a.mem.warps_per_row + (xb >> 5)] + __popc(bal & ((1u << lane) - 1u));
         }
         if ((fl & FL_TYPE) == CT_SOLID) continue;
         float f[Q];
@@ -269,15 +268,14 @@ __global__ void __launch_bounds__(512) k_step(const StepArgs a) {
     }
 }
 
-// The same step for rows whose every node is a pure gather (no solid, no
+// The same step for a row whose every node is a pure gather (no solid, no
 // bounce-back, no curved link; Zou-He allowed) -- the bulk of a domain. Without
-// the rare paths the kernel fits 64 registers, i.e. four 256-thread blocks per SM.
+// the rare paths the kernel fits 64 registers.
 template <int Q, int COLL, int S, bool LES, bool IDX32>
-__global__ void __launch_bounds__(256, 4) k_step_fast(const StepArgs a) {
+__device__ __forceinline__ void step_row_fast(const StepArgs& a, unsigned e) {
     using L = Lat<Q>;
     using C = Codec<S>;
     using T = typename C::T;
-    const unsigned e = a.rows[blockIdx.x];
     const int nx = a.geo.nx, ny = a.geo.ny, nz = a.geo.nz;
     const int y = static_cast<int>(e & 0xffffu), z = static_cast<int>(e >> 16);
     const long long row0 = (static_cast<long long>(z) * ny + y) * nx;
@@ -332,6 +330,86 @@ __global__ void __launch_bounds__(256, 4) k_step_fast(const StepArgs a) {
 #pragma unroll
             for (int q = 0; q < Q; ++q) C::store_stream(out + (q * P + i), f[q], L::w(q));
         }
+    }
+}
+
+// Single lattice: one block per listed row.
+template <int Q, int COLL, int S, bool LES>
+__global__ void __launch_bounds__(512) k_step(const StepArgs a) {
+    step_row<Q, COLL, S, LES>(a, a.rows[blockIdx.x], blockIdx.x);
+}
+
+template <int Q, int COLL, int S, bool LES, bool IDX32>
+__global__ void __launch_bounds__(256, 4) k_step_fast(const StepArgs a) {
+    step_row_fast<Q, COLL, S, LES, IDX32>(a, a.rows[blockIdx.x]);
+}
+
+// ------------------------------------------------------------------ many lattices
+// A batch advances many independent lattices (same Q, collision model and
+// storage; any sizes, parameters and geometry) with one launch per row kind.
+// Each member's step arguments live in device memory; its buffers swap with the
+// batch's step parity, so the table stays valid while the members step together.
+struct BatchDom {
+    StepArgs a;        // fin / fout unused: taken from buf[] by parity
+    void* buf[2];      // the member's two state buffers
+    int cur0;          // index of the buffer holding the state at batch parity 0
+    int gen_first;     // first entry of this member in the general-row list
+};
+
+struct BatchArgs {
+    const BatchDom* dom;
+    const uint2* rows;   // (member, (z << 16) | y), one block per entry
+    int nrows;
+    int parity;          // batch step parity of this launch
+};
+
+__device__ __forceinline__ StepArgs batch_member(const BatchArgs& b, unsigned m) {
+    const BatchDom* d = b.dom + m;
+    StepArgs a = d->a;
+    const int c = d->cur0 ^ b.parity;
+    a.fin = d->buf[c];
+    a.fout = d->buf[c ^ 1];
+    return a;
+}
+
+template <int Q, int COLL, int S, bool LES>
+__global__ void __launch_bounds__(512) k_step_batch(const BatchArgs b) {
+    const uint2 r = b.rows[blockIdx.x];
+    const StepArgs a = batch_member(b, r.x);
+    step_row<Q, COLL, S, LES>(a, r.y, static_cast<int>(blockIdx.x) - b.dom[r.x].gen_first);
+}
+
+template <int Q, int COLL, int S, bool LES, bool IDX32>
+__global__ void __launch_bounds__(256, 4) k_step_fast_batch(const BatchArgs b) {
+    const uint2 r = b.rows[blockIdx.x];
+    const StepArgs a = batch_member(b, r.x);
+    step_row_fast<Q, COLL, S, LES, IDX32>(a, r.y);
+}
+
+// Sum one step's momentum-exchange slots in slot order with one 256-thread block
+// (thread t takes slots t, t + 256, ... in order, then a fixed tree) and append
+// the force to the history ring. Same sum for any launch, so forces are
+// reproducible bit for bit.
+__device__ __forceinline__ void mem_reduce_block(const double* __restrict__ contrib, int n, unsigned* hist_step,
+                                                 double* hist, int hist_cap) {
+    __shared__ double red[3][256];
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int j = threadIdx.x; j < n; j += 256)
+        for (int c = 0; c < 3; ++c) s[c] += contrib[3 * static_cast<long long>(j) + c];
+    for (int c = 0; c < 3; ++c) red[c][threadIdx.x] = s[c];
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            for (int c = 0; c < 3; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const unsigned step = *hist_step;
+        double* h = hist + 3 * static_cast<long long>(step % static_cast<unsigned>(hist_cap));
+        h[0] = red[0][0];
+        h[1] = red[1][0];
+        h[2] = red[2][0];
+        *hist_step = step + 1u;
     }
 }
 

@@ -45,6 +45,9 @@ class _Grid:
     # -- lifetime
     def close(self):
         if getattr(self, "_h", None):
+            batch = getattr(self, "_batch", None)
+            if batch is not None and batch.handle:
+                batch.remove(self)  # a member must leave its batch before it is destroyed
             lib.wake_grid_destroy(self._h)
             self._h = None
 

@@ -113,6 +113,87 @@ def _rasterize_circle(t: np.ndarray, cx: float, cy: float, radius: float) -> Non
                 t[y, x] = SOLID
 
 
+def _rasterize_ellipse(t: np.ndarray, cx: float, cy: float, a: float, b: float, angle: float) -> None:
+    """Rotated ellipse in float32, the rule of wake_grid_set_solid_ellipse (cell centres
+    at integer coordinates; cos/sin evaluated in double and rounded to float)."""
+    ny, nx = t.shape
+    f32 = np.float32
+    r = max(f32(a), f32(b))
+    min_x = max(0, int(f32(cx) - r - f32(1)))
+    max_x = min(nx - 1, int(f32(cx) + r + f32(1)))
+    min_y = max(0, int(f32(cy) - r - f32(1)))
+    max_y = min(ny - 1, int(f32(cy) + r + f32(1)))
+    ang = float(f32(angle))
+    c, s = f32(math.cos(ang)), f32(math.sin(ang))
+    inv_a2 = f32(1.0) / (f32(a) * f32(a))
+    inv_b2 = f32(1.0) / (f32(b) * f32(b))
+    ys = np.arange(min_y, max_y + 1)
+    xs = np.arange(min_x, max_x + 1)
+    Y, X = np.meshgrid(ys, xs, indexing="ij")
+    dx = X.astype(f32) - f32(cx)
+    dy = Y.astype(f32) - f32(cy)
+    u = dx * c + dy * s
+    v = -dx * s + dy * c
+    inside = (u * u * inv_a2 + v * v * inv_b2) <= f32(1.0)
+    sub = t[min_y:max_y + 1, min_x:max_x + 1]
+    sub[inside] = SOLID
+
+
+def ellipse_channel(nx: int, ny: int, a: float, b: float, angle_deg: float, reynolds: float, u_in: float = 0.05,
+                    collision: int = 1, les: bool = True, cs_smag: float = 0.17, noise: float = 1e-4,
+                    seed: int = BASE_SEED, noise_offset: int = 0) -> Case:
+    """2D channel around a rotated ellipse (the batched sweep's domain).
+
+    Layout as cylinder_channel: Zou-He inlet u_in on x = 0, outlet rho = 1 on
+    x = nx-1, solid rows y = 0 and y = ny-1, obstacle centred at (nx/5, ny/2).
+    tau from nu = u_in * 2a / Re (chord 2a). Momentum exchange within 1.5 chords.
+    The Smagorinsky model (Cs = 0.17, as the sphere channel) is on by default: at
+    the sweep's smallest chords tau comes within 0.004 of 1/2 and plain TRT with a
+    Zou-He outlet diverges after ~2,000 steps (oracle and GPU alike).
+    """
+    t = np.zeros((ny, nx), np.uint8)
+    t[:, 0] = INFLOW
+    t[:, nx - 1] = OUTFLOW
+    t[0, :] = SOLID
+    t[ny - 1, :] = SOLID
+    cx, cy = nx / 5.0, ny / 2.0
+    angle = math.radians(angle_deg)
+    _rasterize_ellipse(t, cx, cy, a, b, angle)
+    n = nx * ny
+    r = uniform24(seed, 2 * n, noise_offset)
+    ux = np.float32(u_in) + np.float32(noise) * (np.float32(2.0) * r[:n] - np.float32(1.0))
+    uy = np.float32(noise) * (np.float32(2.0) * r[n:] - np.float32(1.0))
+    nu = u_in * 2.0 * a / reynolds
+    tau = 0.5 + 3.0 * nu
+    return Case(q=9, nx=nx, ny=ny, nz=1, types=t.ravel(), rho=np.ones(n, np.float32), ux=ux.astype(np.float32),
+                uy=uy.astype(np.float32), uz=np.zeros(n, np.float32), tau=tau, collision=collision, les=les,
+                cs_smag=cs_smag, inflow=(u_in, 0.0, 0.0), outflow=1.0, mem=(cx, cy, 0.0, 1.5 * 2.0 * a),
+                ref_area=2.0 * a, u_ref=u_in,
+                extra={"a": a, "b": b, "angle_deg": angle_deg, "re": reynolds, "ellipse": (cx, cy, a, b, angle)})
+
+
+def ellipse_sweep(n_domains: int = 512, nx_range=(64, 512), seed: int = BASE_SEED, collision: int = 1,
+                  first: int = 0, les: bool = True) -> list:
+    """The batched sweep: domain d draws from SplitMix64(seed + d) NX ~ U[nx_range] (integer), NY = NX/2,
+    semi-axes a in [NY/16, NY/6] and b in [max(NY/16, a/3), a] (aspect a/b in [1, 3]), angle of attack
+    ~ U[0, 20] degrees and Re ~ U[50, 300] (outputs 1-5 of the stream), initial noise from output 6 on.
+    Domains first .. first + n_domains - 1."""
+    cases = []
+    for d in range(first, first + n_domains):
+        u = uniform24(seed + d, 5).astype(np.float64)
+        nx = int(nx_range[0] + math.floor(u[0] * (nx_range[1] - nx_range[0] + 1)))
+        ny = nx // 2
+        lo, hi = ny / 16.0, ny / 6.0
+        a = lo + u[1] * (hi - lo)
+        b_lo = max(lo, a / 3.0)
+        b = b_lo + u[2] * (a - b_lo)
+        angle = 20.0 * u[3]
+        re = 50.0 + 250.0 * u[4]
+        cases.append(ellipse_channel(nx, ny, a, b, angle, re, collision=collision, les=les, seed=seed + d,
+                                     noise_offset=5))
+    return cases
+
+
 def sphere_channel(nx=256, ny=128, nz=128, radius=12.0, center=(64.0, 64.0, 64.0), u_in=0.05, tau=0.52,
                    collision=1, les=True, cs_smag=0.17, reference_variant=False) -> Case:
     """3D sphere in a channel.
