@@ -49,6 +49,12 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batch", action="store_true", help="skip the batched ellipse-sweep leg")
     p.add_argument("--batch-only", action="store_true", help="only the batched ellipse-sweep leg (one JSON line)")
+    p.add_argument("--no-serve", action="store_true", help="skip the served-mix leg")
+    p.add_argument("--serve-rate", type=float, default=20.0, help="arrival rate of the served-mix leg (jobs/s)")
+    p.add_argument("--serve-jobs", type=int, default=60, help="jobs in the served-mix leg")
+    p.add_argument("--serve-graph", type=int, default=20, help="steps per CUDA graph inside a served batch (0: plain)")
+    p.add_argument("--serve-sweep", default=None,
+                   help="comma-separated arrival rates: only the served mix at each rate (one JSON line per rate)")
     p.add_argument("--graph", type=int, default=20, help="steps per captured CUDA graph (0: plain launches)")
     p.add_argument("--profile", choices=["f32", "f16", "bf16"], default=None,
                    help="profiling mode: only warm-up + timed steps of this storage, plain launches, one JSON line")
@@ -310,6 +316,33 @@ def batched_leg(storage, n_domains=512, steps=STEPS_PER_SIM, warmup=20, baseline
             "speedup_vs_per_job": sims / base_sims}
 
 
+SERVE_WORKLOAD = ("served mix: Poisson arrivals of D2Q9 channel jobs (ellipse sweep domains, TRT+LES) and D3Q19 "
+                  "sphere jobs (n^3, n~U[48,160], TRT+LES), 50/50, steps lognormal (median 2000, p5 500, clipped "
+                  "200-20000), admission by an HBM budget of 80% of free device memory")
+
+
+def serving_leg(rate, n_jobs, storage="f32", baseline=True, graph_steps=20):
+    """Continuous batching (wake_b200.serve.Server) against one-job-at-a-time plain launches on the same
+    arrival list, both in real time. sims/s = jobs / makespan; latency = completion - arrival."""
+    import torch
+
+    from wake_b200 import serve as S
+
+    jobs = S.mixed_jobs(n_jobs, rate)
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(0.8 * free)
+    rep = S.Server(budget, storage=storage, max_tick_steps=100, graph_steps=graph_steps).run(jobs, realtime=True)
+    out = {"rate_jobs_per_s": rate, "storage": storage, "graph_steps": graph_steps, **rep.summary()}
+    out["mlups"] = out["node_steps"] / max(rep.makespan, 1e-9) / 1e6
+    if baseline:
+        torch.cuda.empty_cache()
+        base = S.run_per_job(jobs, storage=storage, realtime=True).summary()
+        out["per_job_plain"] = {k: base[k] for k in ("sims_per_s", "p50_latency_s", "p99_latency_s", "makespan_s",
+                                                     "failed")}
+        out["speedup_vs_per_job"] = out["sims_per_s"] / max(base["sims_per_s"], 1e-12)
+    return out
+
+
 def reference_sample(case_ref, steps_cap, budget_s, threads=1):
     """Time the reference's own LatticeGrid3D::step + momentum exchange (oracle/_ref) on host cores."""
     import oracle
@@ -386,6 +419,11 @@ def main():
         return
     if args.profile:
         run_profile(args)
+        return
+    if args.serve_sweep:
+        for rate in [float(r) for r in args.serve_sweep.split(",")]:
+            print(json.dumps({"workload": SERVE_WORKLOAD, **serving_leg(rate, args.serve_jobs,
+                                                                          graph_steps=args.serve_graph)}), flush=True)
         return
     if args.batch_only:
         out = {"workload": BATCH_WORKLOAD, "f32": batched_leg("f32"), "f16": batched_leg("f16")}
@@ -477,6 +515,9 @@ def main():
     batched = None
     if not args.no_batch:
         batched = {"workload": BATCH_WORKLOAD, "f32": batched_leg("f32"), "f16": batched_leg("f16")}
+    served = None
+    if not args.no_serve:
+        served = {"workload": SERVE_WORKLOAD, **serving_leg(args.serve_rate, args.serve_jobs)}
     clocks.stop()
 
     # ---- CPU baseline (rank 0, N = 1)
@@ -496,7 +537,7 @@ def main():
                            "l2": "inputs larger than L2 (two 319 MB population buffers, 126 MB L2)",
                            "parallelism": "replicas" if world > 1 else "single GPU",
                            "graph_steps": args.graph, "final_cd": cd},
-                "roofline": roof, "fp16": fp16, "cpu_baseline": cpu, "e2e": e2e, "batched": batched,
+                "roofline": roof, "fp16": fp16, "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "served": served,
                 "clocks": clocks.summary(),
                 "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line))

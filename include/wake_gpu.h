@@ -45,6 +45,12 @@ int wake_gpu_last_error_code(void);
 void wake_gpu_clear_error(void);
 /* Library version string. */
 const char* wake_gpu_version(void);
+/* Device blocks of destroyed grids and batches are kept for reuse instead of
+ * being freed (cudaFree synchronises the whole device). trim frees every cached
+ * block of the current device and returns the bytes freed; cache_bytes reports
+ * what the cache holds. An allocation that fails trims the cache and retries. */
+long long wake_gpu_cache_trim(void);
+long long wake_gpu_cache_bytes(void);
 
 /* ------------------------------------------------- drop-in kernel entry points */
 /* D2Q9: src/ispc/d2q9_collision_bgk.ispc:5-16 */
@@ -208,9 +214,18 @@ int wake_grid_num_curved_links(wake_grid* g);
 int wake_grid_get_curved_links(wake_grid* g, int* fluid_indices, int* q_dirs, float* delta);
 
 /* Initial state: equilibrium of uniform / per-node fields (initialize,
- * initialize_custom), or raw populations f_src [q][node] in host memory. */
+ * initialize_custom: lattice_grid_2d.cpp:64-120), or raw populations f_src
+ * [q][node] in host memory. The equilibrium is evaluated on the device in the
+ * reference's float order; the fields may be host or device arrays. */
 int wake_grid_initialize(wake_grid* g, float rho, float ux, float uy, float uz);
 int wake_grid_initialize_fields(wake_grid* g, const float* rho, const float* ux, const float* uy, const float* uz);
+/* Equilibrium of rho and u + amplitude * (2 r - 1) per component, r the 24-bit
+ * uniform (top 24 bits * 2^-24) of SplitMix64 output offset + 1 + a * N + i
+ * of `seed` for component a of node i, generated on the device. Same bits as
+ * building the noisy fields on the host and calling initialize_fields. No
+ * reference counterpart (the scenarios draw their noise on the host). */
+int wake_grid_initialize_noise(wake_grid* g, float rho, float ux, float uy, float uz, float amplitude,
+                               unsigned long long seed, long long offset);
 int wake_grid_set_populations(wake_grid* g, const float* f /* host [q][nx*ny*nz] */);
 /* Same, from device memory (no host staging). */
 int wake_grid_set_populations_device(wake_grid* g, const float* f_dev /* device [q][nx*ny*nz] */);
@@ -270,8 +285,11 @@ int wake_grid_set_solid_ellipse(wake_grid* g, float cx, float cy, float a, float
 
 /* Device memory: what the grid holds now, and an upper estimate for a new grid
  * of that shape (state buffers, FP32 initialisation scratch, flags, tables and,
- * with with_fields, the macroscopic-field scratch). release_scratch frees the
- * FP32 population and field scratch (re-allocated on demand by the readers).
+ * with with_fields, the macroscopic-field scratch). release_scratch first
+ * completes any pending setup (flags, initial collide), then frees the FP32
+ * population and field scratch (re-allocated on demand by the readers). A
+ * parameter change after it and before the first step re-collides f^0 as held
+ * in the state buffer, i.e. at storage precision.
  * No reference counterpart (the reference allocates host AlignedBuffers,
  * include/wake/core/memory.hpp:52-159). */
 long long wake_grid_device_bytes(wake_grid* g);

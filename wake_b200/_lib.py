@@ -33,6 +33,8 @@ _PROTOS = {
     "wake_gpu_last_error_code": (I, []),
     "wake_gpu_clear_error": (None, []),
     "wake_gpu_version": (C.c_char_p, []),
+    "wake_gpu_cache_trim": (LL, []),
+    "wake_gpu_cache_bytes": (LL, []),
     # drop-in kernels (ISPC signatures)
     "d2q9_collide_bgk": (None, [vp, vp, vp, vp, vp, vp, F, F, F, I]),
     "d2q9_collide_trt": (None, [vp, vp, vp, vp, vp, vp, F, F, F, F, I]),
@@ -87,6 +89,7 @@ _PROTOS = {
     "wake_grid_get_curved_links": (I, [vp, vp, vp, vp]),
     "wake_grid_initialize": (I, [vp, F, F, F, F]),
     "wake_grid_initialize_fields": (I, [vp, vp, vp, vp, vp]),
+    "wake_grid_initialize_noise": (I, [vp, F, F, F, F, F, C.c_ulonglong, LL]),
     "wake_grid_set_populations": (I, [vp, vp]),
     "wake_grid_set_populations_device": (I, [vp, vp]),
     "wake_grid_enable_forces": (I, [vp, F, F, F, F, I]),

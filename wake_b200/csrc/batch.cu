@@ -68,6 +68,12 @@ struct wake_batch {
     unsigned graph_shape = ~0u;
 
     ~wake_batch() {
+        if (stream && cudaStreamSynchronize(stream) == cudaSuccess && (!side || cudaStreamSynchronize(side) == cudaSuccess)) {
+            d_dom.release();
+            d_fast.release();
+            d_gen.release();
+            d_red.release();
+        }
         if (graph) cudaGraphExecDestroy(graph);
         if (own_stream && stream) cudaStreamDestroy(stream);
         if (side) cudaStreamDestroy(side);

@@ -17,7 +17,19 @@ void clear_error();
         if (e_ != cudaSuccess) return ::wk::set_error(-2, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-// Device allocation owned by one object. Nothing is allocated until alloc().
+// Device blocks are taken from, and may be handed back to, a process-wide cache
+// (alloc_cache.cpp). cudaFree synchronises the whole device, so an object whose
+// work is known to be finished (its stream synchronised) returns its blocks with
+// release() instead: a serving loop can then retire jobs and start new ones while
+// other streams keep running, and a new lattice reuses the retired one's memory
+// without a cudaMalloc. reset() keeps the synchronous cudaFree for blocks whose
+// last use is not known to have finished.
+cudaError_t cache_alloc(void** p, std::size_t bytes, std::size_t* block_bytes);
+void cache_release(void* p, std::size_t block_bytes);
+std::size_t cache_trim();         // cudaFree every cached block of the current device; bytes freed
+std::size_t cache_held_bytes();   // bytes held by the cache on the current device
+
+// Device allocation owned by one object. Nothing is allocated until ensure().
 struct DevMem {
     void* p = nullptr;
     std::size_t bytes = 0;
@@ -30,18 +42,24 @@ struct DevMem {
         p = nullptr;
         bytes = 0;
     }
+    // Hand the block to the cache; only when no queued work can still touch it.
+    void release() {
+        if (p) cache_release(p, bytes);
+        p = nullptr;
+        bytes = 0;
+    }
     // (Re)allocate when the current block is smaller than b. Returns cudaSuccess or the error.
     cudaError_t ensure(std::size_t b) {
         if (p && bytes >= b) return cudaSuccess;
         reset();
         if (b == 0) return cudaSuccess;
-        cudaError_t e = cudaMalloc(&p, b);
+        cudaError_t e = cache_alloc(&p, b, &bytes);
         if (e != cudaSuccess) {
             p = nullptr;
+            bytes = 0;
             (void)cudaGetLastError();
             return e;
         }
-        bytes = b;
         return cudaSuccess;
     }
     template <class T>

@@ -124,6 +124,95 @@ __global__ void __launch_bounds__(256) k_mem_reduce(const double* __restrict__ c
     mem_reduce_block(contrib, n, hist_step, hist, hist_cap);
 }
 
+// ---------------------------------------------------------------- device initialisation
+// Initial populations f = feq(rho, u) written straight into the FP32 scratch,
+// in the reference's float order (lattice_grid_2d.cpp:90-119) with every
+// rounding explicit, so they equal the host formula bit for bit. The velocity is
+// uniform, uniform plus seeded noise, or read per node from device arrays.
+struct InitSpec {
+    int mode;                 // 0 uniform, 1 uniform + noise, 2 per-node fields
+    float rho, u[3];
+    float amp;                // noise: u_a += amp * (2 r - 1), r a 24-bit uniform
+    unsigned long long seed;  // SplitMix64 stream; component a of node i takes output offset + 1 + a*N + i
+    long long offset;
+    const float *rho_p, *ux_p, *uy_p, *uz_p;
+};
+
+__device__ __forceinline__ float splitmix_uniform24(unsigned long long seed, unsigned long long i) {
+    // SplitMix64 (Steele, Lea & Flood, OOPSLA 2014): output i of the stream of `seed`, top 24 bits
+    unsigned long long z = seed + i * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return __fmul_rn(static_cast<float>(z >> 40), 5.9604644775390625e-8f);  // * 2^-24
+}
+
+template <int Q>
+__global__ void k_init_eq(float* __restrict__ f, long long pitch, long long n, int dims, InitSpec s) {
+    using L = Lat<Q>;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        float rho = s.rho, u[3] = {s.u[0], s.u[1], s.u[2]};
+        if (s.mode == 2) {
+            rho = s.rho_p[i];
+            u[0] = s.ux_p[i];
+            u[1] = s.uy_p[i];
+            u[2] = (s.uz_p && dims == 3) ? s.uz_p[i] : 0.f;
+        } else if (s.mode == 1) {
+            for (int a = 0; a < dims; ++a) {
+                const float r = splitmix_uniform24(s.seed, static_cast<unsigned long long>(s.offset + 1 + a * n + i));
+                u[a] = __fadd_rn(u[a], __fmul_rn(s.amp, __fsub_rn(__fmul_rn(2.0f, r), 1.0f)));
+            }
+        }
+        const float usq = __fadd_rn(__fadd_rn(__fmul_rn(u[0], u[0]), __fmul_rn(u[1], u[1])), __fmul_rn(u[2], u[2]));
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float cu = __fadd_rn(__fadd_rn(__fmul_rn(float(L::cx(q)), u[0]), __fmul_rn(float(L::cy(q)), u[1])),
+                                       __fmul_rn(float(L::cz(q)), u[2]));
+            float t = __fadd_rn(1.0f, __fmul_rn(3.0f, cu));
+            t = __fadd_rn(t, __fmul_rn(__fmul_rn(4.5f, cu), cu));
+            t = __fsub_rn(t, __fmul_rn(1.5f, usq));
+            f[q * pitch + i] = __fmul_rn(__fmul_rn(L::w(q), rho), t);
+        }
+    }
+}
+
+cudaError_t launch_init_eq(int Q, float* f, long long pitch, long long n, int dims, const InitSpec& s,
+                           cudaStream_t stream) {
+    const int blocks = static_cast<int>(std::min<long long>((n + 255) / 256, 148ll * 16));
+    if (Q == 9) k_init_eq<9><<<blocks, 256, 0, stream>>>(f, pitch, n, dims, s);
+    else if (Q == 19) k_init_eq<19><<<blocks, 256, 0, stream>>>(f, pitch, n, dims, s);
+    else k_init_eq<27><<<blocks, 256, 0, stream>>>(f, pitch, n, dims, s);
+    return cudaGetLastError();
+}
+
+// Fluid nodes with a Solid neighbour (x periodic, y / z in range, no wrap): the
+// candidates of the curved-link builder. Each found node appends (index, direction
+// mask) through one atomic counter; the host sorts the short list by node, so the
+// order of the result does not depend on the launch.
+template <int Q>
+__global__ void k_solid_neighbours(const uint8_t* __restrict__ types, int nx, int ny, int nz,
+                                   unsigned* __restrict__ count, int2* __restrict__ list, unsigned cap) {
+    using L = Lat<Q>;
+    const long long n = static_cast<long long>(nx) * ny * nz;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        if ((types[i] & FL_TYPE) != CT_FLUID) continue;
+        const int x = static_cast<int>(i % nx), y = static_cast<int>((i / nx) % ny), z = static_cast<int>(i / (static_cast<long long>(nx) * ny));
+        int mask = 0;
+#pragma unroll
+        for (int q = 1; q < Q; ++q) {
+            const int xn = (x + L::cx(q) + nx) % nx, yn = y + L::cy(q), zn = z + L::cz(q);
+            if (yn < 0 || yn >= ny || zn < 0 || zn >= nz) continue;
+            if ((types[(static_cast<long long>(zn) * ny + yn) * nx + xn] & FL_TYPE) == CT_SOLID) mask |= 1 << q;
+        }
+        if (mask) {
+            const unsigned slot = atomicAdd(count, 1u);
+            if (slot < cap) list[slot] = make_int2(static_cast<int>(i), mask);
+        }
+    }
+}
+
 cudaError_t launch_link_marks(const int* link_node, int n_links, uint8_t* flags, int* node_start,
                               cudaStream_t stream) {
     if (n_links <= 0) return cudaSuccess;
@@ -232,6 +321,7 @@ int rebuild_flags(wake_grid* g) {
             WK_CUDA(g->d_contrib.ensure(sizeof(double) * 3 * std::max(1, count)));
         }
         WK_CUDA(cudaStreamSynchronize(g->stream));  // the host vectors go out of scope
+        cls.release();
         g->h_fast_rows = std::move(fast);
         g->h_gen_rows = std::move(gen);
     }
@@ -327,8 +417,10 @@ int materialise(wake_grid* g, bool want_f, bool want_macro) {
     }
     if (want_f) WK_CUDA(g->m_f.ensure(sizeof(float) * g->Q * g->pitch));
     const Out o = scratch_out(g, want_f, want_macro);
+    // before the first step the other buffer holds f^0 itself (k_initial), read in place;
+    // after it, f^k is re-gathered from g^{k-1}
     WK_CUDA(launch_materialise_any(g->Q, g->storage, g->buf(1 - g->cur), g->d_flags.as<uint8_t>(), g->geo(),
-                                   g->links(), rp, o, g->launch(), 0));
+                                   g->links(), rp, o, g->launch(), g->k == 0 ? 1 : 0));
     if (want_f) g->mf_valid = true;
     return WAKE_OK;
 }
@@ -370,26 +462,28 @@ int prepare(wake_grid* g) {
     return initial_from_scratch(g);
 }
 
+// The FP32 scratch now holds f^0: the next step collides it (fresh run, step 0).
+void f0_written(wake_grid* g) {
+    g->mf_valid = true;
+    g->pending = true;
+    g->k = 0;
+    g->invalidate_graph();
+}
+
 int upload_f0(wake_grid* g, const float* f, cudaMemcpyKind kind) {
     WK_CUDA(g->m_f.ensure(sizeof(float) * g->Q * g->pitch));
     WK_CUDA(cudaMemcpy2DAsync(g->m_f.p, sizeof(float) * g->pitch, f, sizeof(float) * g->N, sizeof(float) * g->N,
                               g->Q, kind, g->stream));
     WK_CUDA(cudaStreamSynchronize(g->stream));
-    g->mf_valid = true;
-    g->pending = true;
-    g->k = 0;
-    g->invalidate_graph();
+    f0_written(g);
     return WAKE_OK;
 }
 
-// Host equilibrium in the reference's float order (lattice_grid_2d.cpp:90-119):
-// writes f[q * stride] for q = 0..Q-1.
-void equilibrium(const HostLat& lat, float rho, float ux, float uy, float uz, float* f, long long stride) {
-    const float u_sq = ux * ux + uy * uy + uz * uz;
-    for (int q = 0; q < lat.Q; ++q) {
-        const float ci_u = float(lat.cx[q]) * ux + float(lat.cy[q]) * uy + float(lat.cz[q]) * uz;
-        f[q * stride] = lat.w[q] * rho * (1.0f + 3.0f * ci_u + 4.5f * ci_u * ci_u - 1.5f * u_sq);
-    }
+int init_on_device(wake_grid* g, const InitSpec& s) {
+    WK_CUDA(g->m_f.ensure(sizeof(float) * g->Q * g->pitch));
+    WK_CUDA(launch_init_eq(g->Q, g->m_f.as<float>(), g->pitch, g->N, g->D, s, g->stream));
+    f0_written(g);
+    return WAKE_OK;
 }
 
 int do_steps(wake_grid* g, int n) {
@@ -772,36 +866,73 @@ int wake_grid_set_curved_links(wake_grid* g, int n, const int* fluid_indices, co
 int wake_grid_build_curved_sphere_links(wake_grid* g, float cx, float cy, float cz, float radius) {
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
     if (g->Q != 19) return set_error(WAKE_ERR_INVALID, "curved links are D3Q19 only");
+    // candidates on the device: the full-lattice neighbour scan is the costly part of
+    // the reference's host loop; only the few boundary nodes come back
+    const unsigned cap = static_cast<unsigned>(std::min<long long>(g->N, std::max<long long>(4096, g->N / 16)));
+    DevMem d_list, d_count;
+    WK_CUDA(d_list.ensure(sizeof(int2) * cap));
+    WK_CUDA(d_count.ensure(sizeof(unsigned)));
+    WK_CUDA(cudaMemcpyAsync(g->d_types.p, g->types.data(), g->N, cudaMemcpyHostToDevice, g->stream));
+    WK_CUDA(cudaMemsetAsync(d_count.p, 0, sizeof(unsigned), g->stream));
+    const int blocks = static_cast<int>(std::min<long long>((g->N + 255) / 256, 148ll * 16));
+    k_solid_neighbours<19><<<blocks, 256, 0, g->stream>>>(g->d_types.as<uint8_t>(), g->nx, g->ny, g->nz,
+                                                            d_count.as<unsigned>(), d_list.as<int2>(), cap);
+    WK_CUDA(cudaGetLastError());
+    unsigned found = 0;
+    WK_CUDA(cudaMemcpyAsync(&found, d_count.p, sizeof(unsigned), cudaMemcpyDeviceToHost, g->stream));
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    std::vector<int2> cand;
+    if (found <= cap) {
+        cand.resize(found);
+        if (found)
+            WK_CUDA(cudaMemcpyAsync(cand.data(), d_list.p, sizeof(int2) * found, cudaMemcpyDeviceToHost, g->stream));
+        WK_CUDA(cudaStreamSynchronize(g->stream));
+        std::sort(cand.begin(), cand.end(), [](const int2& a, const int2& b) { return a.x < b.x; });
+    } else {
+        // more boundary nodes than the list holds (solid-heavy lattice): scan on the host
+        for (long long i = 0; i < g->N; ++i) {
+            if (g->types[i] != WAKE_CELL_FLUID) continue;
+            const int x = static_cast<int>(i % g->nx), y = static_cast<int>((i / g->nx) % g->ny),
+                      z = static_cast<int>(i / (static_cast<long long>(g->nx) * g->ny));
+            int mask = 0;
+            for (int q = 1; q < 19; ++q) {
+                const int xn = (x + g->lat.cx[q] + g->nx) % g->nx, yn = y + g->lat.cy[q], zn = z + g->lat.cz[q];
+                if (yn < 0 || yn >= g->ny || zn < 0 || zn >= g->nz) continue;
+                if (g->types[idx3(g, xn, yn, zn)] == WAKE_CELL_SOLID) mask |= 1 << q;
+            }
+            if (mask) cand.push_back(make_int2(static_cast<int>(i), mask));
+        }
+    }
+    // delta from the analytic sphere, in the reference's float arithmetic (lattice_grid_3d.cpp:237-256)
     std::vector<int> idx, qd;
     std::vector<float> delta;
-    for (int z = 0; z < g->nz; ++z)
-        for (int y = 0; y < g->ny; ++y)
-            for (int x = 0; x < g->nx; ++x) {
-                if (g->types[idx3(g, x, y, z)] != WAKE_CELL_FLUID) continue;
-                for (int q = 1; q < 19; ++q) {
-                    const int xn = (x + g->lat.cx[q] + g->nx) % g->nx, yn = y + g->lat.cy[q], zn = z + g->lat.cz[q];
-                    if (yn < 0 || yn >= g->ny || zn < 0 || zn >= g->nz) continue;
-                    if (g->types[idx3(g, xn, yn, zn)] != WAKE_CELL_SOLID) continue;
-                    const float px = static_cast<float>(x) - cx, py = static_cast<float>(y) - cy,
-                                pz = static_cast<float>(z) - cz;
-                    const float dx = float(g->lat.cx[q]), dy = float(g->lat.cy[q]), dz = float(g->lat.cz[q]);
-                    const float a = dx * dx + dy * dy + dz * dz;
-                    const float b = 2.0f * (px * dx + py * dy + pz * dz);
-                    const float c = (px * px + py * py + pz * pz) - radius * radius;
-                    const float disc = b * b - 4.0f * a * c;
-                    float d = 0.5f;
-                    if (disc >= 0.0f) {
-                        const float t1 = (-b - std::sqrt(disc)) / (2.0f * a);
-                        const float t2 = (-b + std::sqrt(disc)) / (2.0f * a);
-                        if (t1 >= 0.0f && t1 <= 1.0f) d = t1;
-                        else if (t2 >= 0.0f && t2 <= 1.0f) d = t2;
-                    }
-                    d = std::clamp(d, 0.01f, 0.99f);
-                    idx.push_back(static_cast<int>(idx3(g, x, y, z)));
-                    qd.push_back(q);
-                    delta.push_back(d);
-                }
+    for (const int2& c : cand) {
+        const long long i = c.x;
+        const int x = static_cast<int>(i % g->nx), y = static_cast<int>((i / g->nx) % g->ny),
+                  z = static_cast<int>(i / (static_cast<long long>(g->nx) * g->ny));
+        for (int q = 1; q < 19; ++q) {
+            if (!(c.y & (1 << q))) continue;
+            const float px = static_cast<float>(x) - cx, py = static_cast<float>(y) - cy, pz = static_cast<float>(z) - cz;
+            const float dx = float(g->lat.cx[q]), dy = float(g->lat.cy[q]), dz = float(g->lat.cz[q]);
+            const float a = dx * dx + dy * dy + dz * dz;
+            const float b = 2.0f * (px * dx + py * dy + pz * dz);
+            const float cc = (px * px + py * py + pz * pz) - radius * radius;
+            const float disc = b * b - 4.0f * a * cc;
+            float d = 0.5f;
+            if (disc >= 0.0f) {
+                const float t1 = (-b - std::sqrt(disc)) / (2.0f * a);
+                const float t2 = (-b + std::sqrt(disc)) / (2.0f * a);
+                if (t1 >= 0.0f && t1 <= 1.0f) d = t1;
+                else if (t2 >= 0.0f && t2 <= 1.0f) d = t2;
             }
+            d = std::clamp(d, 0.01f, 0.99f);
+            idx.push_back(static_cast<int>(i));
+            qd.push_back(q);
+            delta.push_back(d);
+        }
+    }
+    d_list.release();
+    d_count.release();
     return wake_grid_set_curved_links(g, static_cast<int>(idx.size()), idx.data(), qd.data(), delta.data(), nullptr,
                                       nullptr, nullptr);
 }
@@ -822,19 +953,51 @@ int wake_grid_get_curved_links(wake_grid* g, int* fluid_indices, int* q_dirs, fl
 
 int wake_grid_initialize(wake_grid* g, float rho, float ux, float uy, float uz) {
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
-    std::vector<float> f(static_cast<std::size_t>(g->Q) * g->N);
-    float one[27];
-    equilibrium(g->lat, rho, ux, uy, (g->D == 3) ? uz : 0.f, one, 1);
-    for (int q = 0; q < g->Q; ++q) std::fill(f.begin() + q * g->N, f.begin() + (q + 1) * g->N, one[q]);
-    return upload_f0(g, f.data(), cudaMemcpyHostToDevice);
+    InitSpec s{};
+    s.mode = 0;
+    s.rho = rho;
+    s.u[0] = ux;
+    s.u[1] = uy;
+    s.u[2] = (g->D == 3) ? uz : 0.f;
+    return init_on_device(g, s);
+}
+
+int wake_grid_initialize_noise(wake_grid* g, float rho, float ux, float uy, float uz, float amplitude,
+                               unsigned long long seed, long long offset) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (offset < 0) return set_error(WAKE_ERR_INVALID, "wake_grid_initialize_noise: negative stream offset");
+    InitSpec s{};
+    s.mode = 1;
+    s.rho = rho;
+    s.u[0] = ux;
+    s.u[1] = uy;
+    s.u[2] = (g->D == 3) ? uz : 0.f;
+    s.amp = amplitude;
+    s.seed = seed;
+    s.offset = offset;
+    return init_on_device(g, s);
 }
 
 int wake_grid_initialize_fields(wake_grid* g, const float* rho, const float* ux, const float* uy, const float* uz) {
     if (!valid_grid(g) || !rho || !ux || !uy) return set_error(WAKE_ERR_INVALID, "null field");
-    std::vector<float> f(static_cast<std::size_t>(g->Q) * g->N);
-    for (long long i = 0; i < g->N; ++i)
-        equilibrium(g->lat, rho[i], ux[i], uy[i], (uz && g->D == 3) ? uz[i] : 0.f, f.data() + i, g->N);
-    return upload_f0(g, f.data(), cudaMemcpyHostToDevice);
+    int r = ensure_macro(g);
+    if (r) return r;
+    const std::size_t b = sizeof(float) * g->N;
+    WK_CUDA(cudaMemcpyAsync(g->m_rho.p, rho, b, cudaMemcpyDefault, g->stream));
+    WK_CUDA(cudaMemcpyAsync(g->m_ux.p, ux, b, cudaMemcpyDefault, g->stream));
+    WK_CUDA(cudaMemcpyAsync(g->m_uy.p, uy, b, cudaMemcpyDefault, g->stream));
+    const bool has_z = uz && g->D == 3;
+    if (has_z) WK_CUDA(cudaMemcpyAsync(g->m_uz.p, uz, b, cudaMemcpyDefault, g->stream));
+    InitSpec s{};
+    s.mode = 2;
+    s.rho_p = g->m_rho.as<float>();
+    s.ux_p = g->m_ux.as<float>();
+    s.uy_p = g->m_uy.as<float>();
+    s.uz_p = has_z ? g->m_uz.as<float>() : nullptr;
+    r = init_on_device(g, s);
+    if (r) return r;
+    WK_CUDA(cudaStreamSynchronize(g->stream));  // the caller may free its arrays on return
+    return WAKE_OK;
 }
 
 int wake_grid_set_populations(wake_grid* g, const float* f) {

@@ -116,6 +116,17 @@ struct wake_grid {
 
     explicit wake_grid(int q) : lat(q) {}
     ~wake_grid() {
+        // every queued use of the blocks ends here, so they go back to the cache
+        // (no device-wide cudaFree while other lattices run)
+        bool idle = true;
+        if (stream) idle = cudaStreamSynchronize(stream) == cudaSuccess;
+        if (side) idle = idle && cudaStreamSynchronize(side) == cudaSuccess;
+        if (idle) {
+            DevMem* all[] = {&A, &B, &d_types, &d_flags, &d_status, &d_nodestart, &d_link_node, &d_link_q,
+                             &d_link_delta, &d_link_mom, &d_counters, &d_hist, &d_warp_base, &d_contrib,
+                             &d_fast_rows, &d_gen_rows, &m_f, &m_rho, &m_ux, &m_uy, &m_uz, &m_speed, &m_diag};
+            for (DevMem* m : all) m->release();
+        }
         for (cudaEvent_t e : t_ev) cudaEventDestroy(e);
         if (graph) cudaGraphExecDestroy(graph);
         if (own_stream && stream) cudaStreamDestroy(stream);

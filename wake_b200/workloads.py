@@ -43,17 +43,24 @@ def uniform24(seed: int, n: int, offset: int = 0) -> np.ndarray:
 
 @dataclass
 class Case:
-    """One lattice with geometry, initial fields and run parameters."""
+    """One lattice with geometry, initial state and run parameters.
+
+    ``init`` describes the initial velocity field, from which the initial
+    populations are the equilibrium (rho, u):
+      ("uniform", rho, (ux, uy, uz))
+      ("noise", rho, (ux, uy, uz), amplitude, seed, offset): u_a + amplitude * (2 r - 1)
+          with r = uniform24 output offset + a*N + i of the seed's stream (component a, node i)
+      ("fields", rho[N], ux[N], uy[N], uz[N])
+    The ``rho`` / ``ux`` / ``uy`` / ``uz`` arrays are built on first use only;
+    ``build_grid`` initialises uniform and noisy states on the device.
+    """
 
     q: int
     nx: int
     ny: int
     nz: int
     types: np.ndarray          # uint8 [N]
-    rho: np.ndarray            # float32 [N]
-    ux: np.ndarray
-    uy: np.ndarray
-    uz: np.ndarray
+    init: tuple
     tau: float
     collision: int
     les: bool = False
@@ -72,6 +79,44 @@ class Case:
     def n(self) -> int:
         return self.nx * self.ny * self.nz
 
+    def fields(self) -> tuple:
+        """(rho, ux, uy, uz) float32 arrays of the initial state."""
+        cached = self.extra.get("_fields")
+        if cached is not None:
+            return cached
+        n, kind = self.n, self.init[0]
+        if kind == "fields":
+            out = tuple(np.ascontiguousarray(a, np.float32).ravel() for a in self.init[1:5])
+        else:
+            rho = np.full(n, self.init[1], np.float32)
+            u = [np.full(n, np.float32(c), np.float32) for c in self.init[2]]
+            if kind == "noise":
+                amp, seed, off = self.init[3], self.init[4], self.init[5]
+                dims = 3 if self.q != 9 else 2
+                r = uniform24(seed, dims * n, off)
+                for a in range(dims):
+                    u[a] = (np.float32(self.init[2][a]) + np.float32(amp) *
+                            (np.float32(2.0) * r[a * n:(a + 1) * n] - np.float32(1.0))).astype(np.float32)
+            out = (rho, u[0], u[1], u[2])
+        self.extra["_fields"] = out
+        return out
+
+    @property
+    def rho(self) -> np.ndarray:
+        return self.fields()[0]
+
+    @property
+    def ux(self) -> np.ndarray:
+        return self.fields()[1]
+
+    @property
+    def uy(self) -> np.ndarray:
+        return self.fields()[2]
+
+    @property
+    def uz(self) -> np.ndarray:
+        return self.fields()[3]
+
 
 def cylinder_channel(nx=400, ny=160, diameter=20.0, cx=80.0, cy=80.0, u_in=0.05, tau=0.56, collision=0,
                      noise=1e-4, seed=BASE_SEED) -> Case:
@@ -86,12 +131,8 @@ def cylinder_channel(nx=400, ny=160, diameter=20.0, cx=80.0, cy=80.0, u_in=0.05,
     t[0, :] = SOLID
     t[ny - 1, :] = SOLID
     _rasterize_circle(t, cx, cy, diameter * 0.5)
-    n = nx * ny
-    r = uniform24(seed, 2 * n)
-    ux = np.float32(u_in) + np.float32(noise) * (np.float32(2.0) * r[:n] - np.float32(1.0))
-    uy = np.float32(noise) * (np.float32(2.0) * r[n:] - np.float32(1.0))
-    return Case(q=9, nx=nx, ny=ny, nz=1, types=t.ravel(), rho=np.ones(n, np.float32), ux=ux.astype(np.float32),
-                uy=uy.astype(np.float32), uz=np.zeros(n, np.float32), tau=tau, collision=collision,
+    return Case(q=9, nx=nx, ny=ny, nz=1, types=t.ravel(), init=("noise", 1.0, (u_in, 0.0, 0.0), noise, seed, 0),
+                tau=tau, collision=collision,
                 inflow=(u_in, 0.0, 0.0), outflow=1.0, mem=(cx, cy, 0.0, 1.5 * diameter), ref_area=diameter,
                 u_ref=u_in)
 
@@ -159,17 +200,19 @@ def ellipse_channel(nx: int, ny: int, a: float, b: float, angle_deg: float, reyn
     cx, cy = nx / 5.0, ny / 2.0
     angle = math.radians(angle_deg)
     _rasterize_ellipse(t, cx, cy, a, b, angle)
-    n = nx * ny
-    r = uniform24(seed, 2 * n, noise_offset)
-    ux = np.float32(u_in) + np.float32(noise) * (np.float32(2.0) * r[:n] - np.float32(1.0))
-    uy = np.float32(noise) * (np.float32(2.0) * r[n:] - np.float32(1.0))
     nu = u_in * 2.0 * a / reynolds
     tau = 0.5 + 3.0 * nu
-    return Case(q=9, nx=nx, ny=ny, nz=1, types=t.ravel(), rho=np.ones(n, np.float32), ux=ux.astype(np.float32),
-                uy=uy.astype(np.float32), uz=np.zeros(n, np.float32), tau=tau, collision=collision, les=les,
+    return Case(q=9, nx=nx, ny=ny, nz=1, types=t.ravel(),
+                init=("noise", 1.0, (u_in, 0.0, 0.0), noise, seed, noise_offset), tau=tau, collision=collision, les=les,
                 cs_smag=cs_smag, inflow=(u_in, 0.0, 0.0), outflow=1.0, mem=(cx, cy, 0.0, 1.5 * 2.0 * a),
                 ref_area=2.0 * a, u_ref=u_in,
                 extra={"a": a, "b": b, "angle_deg": angle_deg, "re": reynolds, "ellipse": (cx, cy, a, b, angle)})
+
+
+def ellipse_sweep_dims(d: int, nx_range=(64, 512), seed: int = BASE_SEED) -> int:
+    """NX of the sweep's domain d without building it (ellipse_sweep's first draw)."""
+    u0 = float(uniform24(seed + d, 1)[0])
+    return int(nx_range[0] + math.floor(u0 * (nx_range[1] - nx_range[0] + 1)))
 
 
 def ellipse_sweep(n_domains: int = 512, nx_range=(64, 512), seed: int = BASE_SEED, collision: int = 1,
@@ -210,9 +253,7 @@ def sphere_channel(nx=256, ny=128, nz=128, radius=12.0, center=(64.0, 64.0, 64.0
         t[:, :, 0] = np.where(t[:, :, 0] == SOLID, SOLID, INFLOW)
         t[:, :, nx - 1] = np.where(t[:, :, nx - 1] == SOLID, SOLID, OUTFLOW)
         inflow, outflow = (u_in, 0.0, 0.0), 1.0
-    n = nx * ny * nz
-    return Case(q=19, nx=nx, ny=ny, nz=nz, types=t.ravel(), rho=np.ones(n, np.float32),
-                ux=np.full(n, u_in, np.float32), uy=np.zeros(n, np.float32), uz=np.zeros(n, np.float32), tau=tau,
+    return Case(q=19, nx=nx, ny=ny, nz=nz, types=t.ravel(), init=("uniform", 1.0, (u_in, 0.0, 0.0)), tau=tau,
                 collision=collision, les=les and not reference_variant, cs_smag=cs_smag, inflow=inflow,
                 outflow=outflow, periodic_y=not reference_variant, periodic_z=not reference_variant,
                 sphere=(cx, cy, cz, radius), mem=(cx, cy, cz, 2.0 * radius), ref_area=math.pi * radius * radius,
@@ -250,8 +291,9 @@ def taylor_green(L=384, u0=0.04, tau=0.51, q=27, collision=2) -> Case:
     p = (u0 * u0 / 16.0) * (c2[None, None, :] + c2[None, :, None]) * (c2[:, None, None] + 2.0)
     rho = (1.0 + 3.0 * p).astype(np.float32)
     n = L ** 3
-    return Case(q=q, nx=L, ny=L, nz=L, types=np.zeros(n, np.uint8), rho=rho.ravel(), ux=ux.ravel(), uy=uy.ravel(),
-                uz=np.zeros(n, np.float32), tau=tau, collision=collision, periodic_y=True, periodic_z=True,
+    return Case(q=q, nx=L, ny=L, nz=L, types=np.zeros(n, np.uint8),
+                init=("fields", rho.ravel(), ux.ravel(), uy.ravel(), np.zeros(n, np.float32)), tau=tau,
+                collision=collision, periodic_y=True, periodic_z=True,
                 u_ref=u0, extra={"u0": u0, "k": k})
 
 
@@ -265,7 +307,14 @@ def build_grid(case: Case, storage: str = "f32", les_applies: bool = True):
         g = wb.LatticeGrid3D(case.nx, case.ny, case.nz, case.tau, storage=storage, les_applies=les_applies)
     else:
         g = wb.LatticeGrid3DQ27(case.nx, case.ny, case.nz, case.tau, storage=storage, les_applies=les_applies)
-    g.initialize_fields(case.rho, case.ux, case.uy, case.uz if case.q != 9 else None)
+    kind = case.init[0]
+    if kind == "uniform":
+        wb.check(wb.lib.wake_grid_initialize(g.handle, case.init[1], *case.init[2]))
+    elif kind == "noise":
+        _, rho0, u0, amp, seed, off = case.init
+        wb.check(wb.lib.wake_grid_initialize_noise(g.handle, rho0, *u0, amp, seed, off))
+    else:
+        g.initialize_fields(case.rho, case.ux, case.uy, case.uz if case.q != 9 else None)
     g.set_cell_types(case.types)
     if case.q != 9 and (case.periodic_y or case.periodic_z):
         g.set_periodic_axes(case.periodic_y, case.periodic_z)
