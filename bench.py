@@ -59,6 +59,7 @@ def parse():
     p.add_argument("--profile", choices=["f32", "f16", "bf16"], default=None,
                    help="profiling mode: only warm-up + timed steps of this storage, plain launches, one JSON line")
     p.add_argument("--block", type=int, default=0, help="threads per block of the fused step (0: automatic)")
+    p.add_argument("--kernel", type=int, default=0, help="pure-gather row kernel: 0 auto, 1 direct gather, 2 staged")
     return p.parse_args()
 
 
@@ -74,10 +75,12 @@ def run_profile(args):
     g = W.build_grid(case, storage=args.profile)
     if args.block:
         wb.check(wb.lib.wake_grid_set_block(g.handle, args.block))
+    wb.check(wb.lib.wake_grid_set_kernel(g.handle, args.kernel))
     if args.graph:
         g.use_graph(args.graph)
     ms = timed_steps(g, case, args.steps, args.warmup, 1)
-    print(json.dumps({"profile": args.profile, "block": wb.lib.wake_grid_get_block(g.handle), "steps": args.steps,
+    print(json.dumps({"profile": args.profile, "kernel": wb.lib.wake_grid_get_kernel(g.handle),
+                      "block": wb.lib.wake_grid_get_block(g.handle), "steps": args.steps,
                       "ms_per_step": ms / args.steps, "mlups": case.n * args.steps / (ms * 1e-3) / 1e6}))
     torch.cuda.synchronize()
 

@@ -267,6 +267,16 @@ void* wake_grid_state_buffer(wake_grid* g, int which);
 /* Launch shape of the fused kernel: threads per block (32..512, multiple of 32). */
 int wake_grid_set_block(wake_grid* g, int threads_per_block);
 int wake_grid_get_block(wake_grid* g);
+/* Step kernels: 0 automatic (default), 1 direct (a launch over the pure-gather
+ * rows reading global memory, beside a launch over the remaining rows), 2 one
+ * persistent launch per step that stages the pure-gather rows in shared memory
+ * by bulk copies, tiles of up to 1024 nodes, and runs the remaining rows beside
+ * them (used when a row is a whole number of 16-byte chunks and at most 1024
+ * nodes; otherwise the direct kernels run). get_kernel returns the kernels in
+ * use (1 or 2). For TRT both compute two nodes per thread in packed FP32 with
+ * the same roundings. No reference counterpart. */
+int wake_grid_set_kernel(wake_grid* g, int variant);
+int wake_grid_get_kernel(wake_grid* g);
 /* Kernel launches one fused step issues with the current geometry (pure-gather
  * rows, general rows, momentum-exchange reduction). No reference counterpart. */
 int wake_grid_launches_per_step(wake_grid* g);
@@ -317,6 +327,8 @@ int wake_batch_set_stream(wake_batch* b, void* stream);
 int wake_batch_use_graph(wake_batch* b, int steps_per_graph);
 int wake_batch_set_block(wake_batch* b, int threads_bulk, int threads_general);
 int wake_batch_get_block(wake_batch* b);
+/* As wake_grid_set_kernel, for the batch (persistent tiles only when every member allows them). */
+int wake_batch_set_kernel(wake_batch* b, int variant);
 int wake_batch_step(wake_batch* b, int n);
 int wake_batch_synchronize(wake_batch* b);        /* first member error, if any */
 int wake_batch_info(wake_batch* b, long long* nodes, int* bulk_rows, int* general_rows, int* launches_per_step);

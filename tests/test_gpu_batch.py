@@ -51,11 +51,12 @@ def _sweep(n, seed_first=0):
     return W.ellipse_sweep(n, nx_range=(64, 160), first=seed_first)
 
 
-@pytest.mark.parametrize("graph", [0, 10])
-def test_batch_equals_alone_d2q9(graph):
-    cases = _sweep(6)
+@pytest.mark.parametrize("graph,kernel", [(0, 1), (10, 1), (10, 2)])
+def test_batch_equals_alone_d2q9(graph, kernel):
+    cases = [c for c in _sweep(12) if kernel == 1 or c.nx % 4 == 0][:6]
     steps = 47
     b = Batch(9, "f32")
+    wb.check(wb.lib.wake_batch_set_kernel(b.handle, kernel))
     grids = [W.build_grid(c) for c in cases]
     for g, c in zip(grids, cases):
         _add(b, g, c)

@@ -109,6 +109,9 @@ _PROTOS = {
     "wake_grid_set_block": (I, [vp, I]),
     "wake_grid_get_block": (I, [vp]),
     "wake_grid_launches_per_step": (I, [vp]),
+    "wake_grid_set_kernel": (I, [vp, I]),
+    "wake_grid_get_kernel": (I, [vp]),
+    "wake_batch_set_kernel": (I, [vp, I]),
     "wake_grid_time_bulk_launches": (I, [vp, I]),
     "wake_grid_bulk_launch_times": (I, [vp, vp, vp, vp]),
     "wake_grid_set_solid_ellipse": (I, [vp, F, F, F, F, F]),

@@ -53,6 +53,10 @@ struct wake_batch {
     std::vector<MemRed> up_red;
     int n_fast = 0, n_gen = 0, n_red = 0;
     bool idx32 = true;
+    bool tiles = false;      // one persistent tile launch per step (k_step_tiles)
+    int kernel_variant = 0;  // 0 automatic, 1 direct, 2 persistent tiles (when every member allows it)
+    DevMem d_tiles, d_gen4, d_mixed;  // tiles, general segments with entries, spans outside the tiles
+    int n_tiles = 0, n_tile_gen = 0, n_mixed = 0;
     int coll = 0, les = 0;
     int parity = 0;  // batch steps taken, mod 2
 
@@ -73,6 +77,9 @@ struct wake_batch {
             d_fast.release();
             d_gen.release();
             d_red.release();
+            d_tiles.release();
+            d_gen4.release();
+            d_mixed.release();
         }
         if (graph) cudaGraphExecDestroy(graph);
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -103,18 +110,38 @@ int build_rows(wake_batch* b) {
     layout.reserve(b->members.size());
     for (const auto& m : b->members) layout.emplace_back(m.g, m.g->geom_version);
     if (layout == b->layout && b->gen_first.size() == b->members.size()) return WAKE_OK;
-    std::vector<uint2> fast, gen;
+    std::vector<uint4> fast, tiles, gen4, mixed;
+    std::vector<uint2> gen;
     b->gen_first.assign(b->members.size(), 0);
     for (std::size_t i = 0; i < b->members.size(); ++i) {
         const wake_grid* g = b->members[i].g;
-        for (unsigned r : g->h_fast_rows) fast.push_back(make_uint2(static_cast<unsigned>(i), r));
+        const unsigned m = static_cast<unsigned>(i);
+        for (uint4 sp : g->h_fast_rows) fast.push_back(make_uint4(m, sp.y, sp.z, sp.w));
         b->gen_first[i] = static_cast<int>(gen.size());
-        for (unsigned r : g->h_gen_rows) gen.push_back(make_uint2(static_cast<unsigned>(i), r));
+        for (unsigned r : g->h_gen_rows) gen.push_back(make_uint2(m, r));
+        for (uint4 t : g->h_tiles) tiles.push_back(make_uint4(m, t.y, t.z, 0u));
+        for (uint4 t : g->h_gen4) gen4.push_back(make_uint4(m, t.y, t.z, 0u));
+        for (uint4 sp : g->h_mixed) mixed.push_back(make_uint4(m, sp.y, sp.z, sp.w));
     }
-    WK_CUDA(b->d_fast.ensure(sizeof(uint2) * std::max<std::size_t>(1, fast.size())));
+    WK_CUDA(b->d_mixed.ensure(sizeof(uint4) * std::max<std::size_t>(1, mixed.size())));
+    if (!mixed.empty())
+        WK_CUDA(cudaMemcpyAsync(b->d_mixed.p, mixed.data(), sizeof(uint4) * mixed.size(), cudaMemcpyHostToDevice,
+                                b->stream));
+    b->n_mixed = static_cast<int>(mixed.size());
+    WK_CUDA(b->d_tiles.ensure(sizeof(uint4) * std::max<std::size_t>(1, tiles.size())));
+    WK_CUDA(b->d_gen4.ensure(sizeof(uint4) * std::max<std::size_t>(1, gen4.size())));
+    if (!tiles.empty())
+        WK_CUDA(cudaMemcpyAsync(b->d_tiles.p, tiles.data(), sizeof(uint4) * tiles.size(), cudaMemcpyHostToDevice,
+                                b->stream));
+    if (!gen4.empty())
+        WK_CUDA(cudaMemcpyAsync(b->d_gen4.p, gen4.data(), sizeof(uint4) * gen4.size(), cudaMemcpyHostToDevice,
+                                b->stream));
+    b->n_tiles = static_cast<int>(tiles.size());
+    b->n_tile_gen = static_cast<int>(gen4.size());
+    WK_CUDA(b->d_fast.ensure(sizeof(uint4) * std::max<std::size_t>(1, fast.size())));
     WK_CUDA(b->d_gen.ensure(sizeof(uint2) * std::max<std::size_t>(1, gen.size())));
     if (!fast.empty())
-        WK_CUDA(cudaMemcpyAsync(b->d_fast.p, fast.data(), sizeof(uint2) * fast.size(), cudaMemcpyHostToDevice, b->stream));
+        WK_CUDA(cudaMemcpyAsync(b->d_fast.p, fast.data(), sizeof(uint4) * fast.size(), cudaMemcpyHostToDevice, b->stream));
     if (!gen.empty())
         WK_CUDA(cudaMemcpyAsync(b->d_gen.p, gen.data(), sizeof(uint2) * gen.size(), cudaMemcpyHostToDevice, b->stream));
     WK_CUDA(cudaStreamSynchronize(b->stream));  // the host vectors go out of scope
@@ -132,8 +159,10 @@ int build_tables(wake_batch* b) {
     std::vector<BatchDom> dom(n);
     std::vector<MemRed> red;
     b->idx32 = true;
+    bool tiles = b->kernel_variant == 2 && n > 0;
     for (std::size_t i = 0; i < n; ++i) {
         wake_grid* g = b->members[i].g;
+        tiles = tiles && tile_row_ok(g->nx, static_cast<int>(g->elem));
         BatchDom d;
         std::memset(&d, 0, sizeof d);
         d.a = grid_step_args(g);
@@ -153,6 +182,10 @@ int build_tables(wake_batch* b) {
             m.hist_cap = d.a.mem.hist_cap;
             red.push_back(m);
         }
+    }
+    if (tiles != b->tiles) {
+        b->tiles = tiles;
+        ++b->shape;  // a captured graph holds the other kernel
     }
     const bool same_dom = dom.size() == b->up_dom.size() &&
                           (dom.empty() || std::memcmp(dom.data(), b->up_dom.data(), sizeof(BatchDom) * n) == 0);
@@ -177,9 +210,23 @@ int build_tables(wake_batch* b) {
 }
 
 int batch_steps(wake_batch* b, int n) {
+    if (b->tiles) {
+        for (int s = 0; s < n; ++s) {
+            const TileArgs t{b->d_tiles.as<uint4>(), b->n_tiles, b->d_gen4.as<uint4>(), b->n_tile_gen,
+                             b->d_dom.as<BatchDom>(), b->parity, b->d_mixed.as<uint4>(), b->n_mixed};
+            StepArgs unused{};
+            WK_CUDA(launch_tiles_any(b->Q, b->coll, b->storage, b->les != 0, unused, t, b->stream));
+            if (b->n_red > 0) {
+                k_batch_mem_reduce<<<b->n_red, 256, 0, b->stream>>>(b->d_red.as<MemRed>());
+                WK_CUDA(cudaGetLastError());
+            }
+            b->parity ^= 1;
+        }
+        return WAKE_OK;
+    }
     for (int s = 0; s < n; ++s) {
-        BatchArgs fa{b->d_dom.as<BatchDom>(), b->d_fast.as<uint2>(), b->n_fast, b->parity};
-        BatchArgs ga{b->d_dom.as<BatchDom>(), b->d_gen.as<uint2>(), b->n_gen, b->parity};
+        BatchArgs fa{b->d_dom.as<BatchDom>(), nullptr, 0, b->parity, b->d_fast.as<uint4>(), b->n_fast};
+        BatchArgs ga{b->d_dom.as<BatchDom>(), b->d_gen.as<uint2>(), b->n_gen, b->parity, nullptr, 0};
         const bool fork = b->n_fast > 0 && (b->n_gen > 0 || b->n_red > 0);
         cudaStream_t side = fork ? b->side : b->stream;
         if (fork) {
@@ -326,6 +373,15 @@ int wake_batch_set_block(wake_batch* b, int threads_bulk, int threads_general) {
 
 int wake_batch_get_block(wake_batch* b) { return valid_batch(b) ? b->tpb_fast : WAKE_ERR_INVALID; }
 
+int wake_batch_set_kernel(wake_batch* b, int variant) {
+    if (!valid_batch(b)) return WAKE_ERR_INVALID;
+    if (variant < 0 || variant > 2) return set_error(WAKE_ERR_INVALID, "wake_batch_set_kernel: variant 0, 1 or 2");
+    b->kernel_variant = variant;
+    b->up_dom.clear();  // re-evaluated with the tables
+    b->drop_graph();
+    return WAKE_OK;
+}
+
 int wake_batch_step(wake_batch* b, int n) {
     if (!valid_batch(b)) return WAKE_ERR_INVALID;
     if (n < 0) return set_error(WAKE_ERR_INVALID, "negative step count");
@@ -386,7 +442,8 @@ int wake_batch_info(wake_batch* b, long long* nodes, int* bulk_rows, int* genera
     if (nodes) *nodes = nn;
     if (bulk_rows) *bulk_rows = b->n_fast;
     if (general_rows) *general_rows = b->n_gen;
-    if (launches_per_step) *launches_per_step = (b->n_fast > 0) + (b->n_gen > 0) + (b->n_red > 0);
+    if (launches_per_step)
+        *launches_per_step = b->tiles ? 1 + (b->n_red > 0) : (b->n_fast > 0) + (b->n_gen > 0) + (b->n_red > 0);
     return WAKE_OK;
 }
 

@@ -43,6 +43,12 @@ cudaError_t launch_batch_any(int Q, int coll, int store, bool les, const BatchAr
     if (Q == 19) return launch_batch_q19(coll, store, les, b, tpb, stream, fast, idx32);
     return launch_batch_q27(coll, store, les, b, tpb, stream, fast, idx32);
 }
+cudaError_t launch_tiles_any(int Q, int coll, int store, bool les, const StepArgs& a, const TileArgs& t,
+                             cudaStream_t stream) {
+    if (Q == 9) return launch_tiles_q9(coll, store, les, a, t, stream);
+    if (Q == 19) return launch_tiles_q19(coll, store, les, a, t, stream);
+    return launch_tiles_q27(coll, store, les, a, t, stream);
+}
 cudaError_t launch_initial_any(int Q, int coll, int store, bool les, const float* f0, void* a, void* b,
                                const uint8_t* flags, const Geo& geo, const Physics& phys, const Launch& L) {
     if (Q == 9) return launch_initial_q9(coll, store, les, f0, a, b, flags, geo, phys, L);
@@ -62,10 +68,11 @@ cudaError_t launch_flags_any(int Q, const uint8_t* types, uint8_t* flags, const 
     if (Q == 19) return launch_flags_q19(types, flags, geo, cfg, L);
     return launch_flags_q27(types, flags, geo, cfg, L);
 }
-cudaError_t launch_row_class_any(int Q, const uint8_t* flags, uint8_t* cls, const Geo& geo, const Launch& L) {
-    if (Q == 9) return launch_row_class_q9(flags, cls, geo, L);
-    if (Q == 19) return launch_row_class_q19(flags, cls, geo, L);
-    return launch_row_class_q27(flags, cls, geo, L);
+cudaError_t launch_seg_class_any(int Q, const uint8_t* flags, uint8_t* cls, const Geo& geo, long long nsegs,
+                                 cudaStream_t stream) {
+    if (Q == 9) return launch_seg_class_q9(flags, cls, geo, nsegs, stream);
+    if (Q == 19) return launch_seg_class_q19(flags, cls, geo, nsegs, stream);
+    return launch_seg_class_q27(flags, cls, geo, nsegs, stream);
 }
 
 // ---------------------------------------------------------------- small kernels
@@ -266,39 +273,60 @@ int rebuild_flags(wake_grid* g) {
         WK_CUDA(launch_link_marks(g->d_link_node.as<int>(), nl, g->d_flags.as<uint8_t>(), g->d_nodestart.as<int>(),
                                   g->stream));
     }
-    // split the rows between the two step kernels
+    // split the rows into SEG-node segments for the two step kernels
     {
-        const int nr = g->rows;
+        const int nseg = (g->nx + SEG - 1) / SEG;
+        const long long nsegs = static_cast<long long>(g->rows) * nseg;
+        if (nsegs >= (1ll << 32)) return set_error(WAKE_ERR_INVALID, "lattice too large for 32-bit segment numbers");
         DevMem cls;
-        WK_CUDA(cls.ensure(nr));
-        WK_CUDA(launch_row_class_any(g->Q, g->d_flags.as<uint8_t>(), cls.as<uint8_t>(), geo, g->launch()));
-        std::vector<uint8_t> h(nr);
-        WK_CUDA(cudaMemcpyAsync(h.data(), cls.p, nr, cudaMemcpyDeviceToHost, g->stream));
+        WK_CUDA(cls.ensure(static_cast<std::size_t>(nsegs)));
+        WK_CUDA(launch_seg_class_any(g->Q, g->d_flags.as<uint8_t>(), cls.as<uint8_t>(), geo, nsegs, g->stream));
+        std::vector<uint8_t> h(static_cast<std::size_t>(nsegs));
+        WK_CUDA(cudaMemcpyAsync(h.data(), cls.p, h.size(), cudaMemcpyDeviceToHost, g->stream));
         WK_CUDA(cudaStreamSynchronize(g->stream));
-        std::vector<unsigned> fast, gen;
-        std::vector<int> gen_row;  // row index of each general entry
-        for (int r = 0; r < nr; ++r) {
-            const unsigned packed = (static_cast<unsigned>(r / g->ny) << 16) | static_cast<unsigned>(r % g->ny);
-            if (h[r] & 1) {
-                fast.push_back(packed);
-            } else {
-                gen.push_back(packed);
-                gen_row.push_back(r);
+        cls.release();
+        // general segments; pure-gather spans: whole rows, or the runs of pure-gather
+        // segments of the rows that hold general segments
+        std::vector<unsigned> gen;
+        std::vector<uint4> spans, mixed_spans;
+        std::vector<uint8_t> row_fast(static_cast<std::size_t>(g->rows), 1);
+        for (long long e = 0; e < nsegs; ++e) {
+            if (h[e] & 1) continue;
+            gen.push_back(static_cast<unsigned>(e));
+            row_fast[static_cast<std::size_t>(e / nseg)] = 0;
+        }
+        for (int r = 0; r < g->rows; ++r) {
+            if (row_fast[r]) {
+                spans.push_back(make_uint4(0u, static_cast<unsigned>(r), 0u, static_cast<unsigned>(g->nx)));
+                continue;
+            }
+            for (int sg = 0; sg < nseg;) {
+                if (!(h[static_cast<long long>(r) * nseg + sg] & 1)) {
+                    ++sg;
+                    continue;
+                }
+                int s1 = sg + 1;
+                while (s1 < nseg && (h[static_cast<long long>(r) * nseg + s1] & 1)) ++s1;
+                const uint4 sp = make_uint4(0u, static_cast<unsigned>(r), static_cast<unsigned>(sg * SEG),
+                                            static_cast<unsigned>(std::min(g->nx, s1 * SEG)));
+                spans.push_back(sp);
+                mixed_spans.push_back(sp);
+                sg = s1;
             }
         }
-        g->n_fast = static_cast<int>(fast.size());
+        g->n_fast = static_cast<int>(spans.size());
         g->n_gen = static_cast<int>(gen.size());
-        WK_CUDA(g->d_fast_rows.ensure(sizeof(unsigned) * std::max<std::size_t>(1, fast.size())));
+        WK_CUDA(g->d_fast_rows.ensure(sizeof(uint4) * std::max<std::size_t>(1, spans.size())));
         WK_CUDA(g->d_gen_rows.ensure(sizeof(unsigned) * std::max<std::size_t>(1, gen.size())));
-        if (!fast.empty())
-            WK_CUDA(cudaMemcpyAsync(g->d_fast_rows.p, fast.data(), sizeof(unsigned) * fast.size(),
+        if (!spans.empty())
+            WK_CUDA(cudaMemcpyAsync(g->d_fast_rows.p, spans.data(), sizeof(uint4) * spans.size(),
                                     cudaMemcpyHostToDevice, g->stream));
         if (!gen.empty())
             WK_CUDA(cudaMemcpyAsync(g->d_gen_rows.p, gen.data(), sizeof(unsigned) * gen.size(), cudaMemcpyHostToDevice,
                                     g->stream));
-        // momentum-exchange slots: per general row and 32-wide chunk, the number of
+        // momentum-exchange slots: per general segment and 32-node chunk, the number of
         // FL_MEM nodes before it (node order), so slots are dense and ordered
-        g->warps_per_row = (g->nx + 31) / 32;
+        g->warps_per_row = SEG / 32;
         g->n_mem_nodes = 0;
         std::vector<int> warp_base;
         if (g->mem_on) {
@@ -307,11 +335,12 @@ int rebuild_flags(wake_grid* g) {
             WK_CUDA(cudaStreamSynchronize(g->stream));
             warp_base.assign(std::max<std::size_t>(1, gen.size() * g->warps_per_row), 0);
             int count = 0;
-            for (std::size_t e = 0; e < gen.size(); ++e) {
-                const long long row0 = static_cast<long long>(gen_row[e]) * g->nx;
+            for (std::size_t k = 0; k < gen.size(); ++k) {
+                const long long row = gen[k] / nseg, x0 = (gen[k] % nseg) * SEG;
                 for (int c = 0; c < g->warps_per_row; ++c) {
-                    warp_base[e * g->warps_per_row + c] = count;
-                    for (int x = 32 * c; x < std::min(g->nx, 32 * c + 32); ++x) count += (fl[row0 + x] & FL_MEM) ? 1 : 0;
+                    warp_base[k * g->warps_per_row + c] = count;
+                    const long long xa = x0 + 32 * c, xe = std::min<long long>(g->nx, xa + 32);
+                    for (long long x = xa; x < xe; ++x) count += (fl[row * g->nx + x] & FL_MEM) ? 1 : 0;
                 }
             }
             g->n_mem_nodes = count;
@@ -320,9 +349,47 @@ int rebuild_flags(wake_grid* g) {
                                     cudaMemcpyHostToDevice, g->stream));
             WK_CUDA(g->d_contrib.ensure(sizeof(double) * 3 * std::max(1, count)));
         }
-        WK_CUDA(cudaStreamSynchronize(g->stream));  // the host vectors go out of scope
-        cls.release();
-        g->h_fast_rows = std::move(fast);
+        // persistent-kernel work: tiles of consecutive all-pure-gather rows of one z plane
+        // (at most TILE_NODES nodes), the general segments with their slot entry, and the
+        // pure-gather runs of the other rows
+        {
+            const int per_tile = std::max(1, TILE_NODES / g->nx);
+            std::vector<uint4> tiles, gen4;
+            for (int r = 0; r < g->rows;) {
+                if (!row_fast[r]) {
+                    ++r;
+                    continue;
+                }
+                const int z = r / g->ny, y0 = r % g->ny;
+                int cnt = 1;
+                while (cnt < per_tile && r + cnt < g->rows && row_fast[r + cnt] && (r + cnt) / g->ny == z) ++cnt;
+                tiles.push_back(make_uint4(0u, (static_cast<unsigned>(z) << 16) | static_cast<unsigned>(y0),
+                                           static_cast<unsigned>(cnt), 0u));
+                r += cnt;
+            }
+            for (std::size_t k = 0; k < gen.size(); ++k)
+                gen4.push_back(make_uint4(0u, gen[k], static_cast<unsigned>(k), 0u));
+            WK_CUDA(g->d_tiles.ensure(sizeof(uint4) * std::max<std::size_t>(1, tiles.size())));
+            WK_CUDA(g->d_gen4.ensure(sizeof(uint4) * std::max<std::size_t>(1, gen4.size())));
+            WK_CUDA(g->d_mixed.ensure(sizeof(uint4) * std::max<std::size_t>(1, mixed_spans.size())));
+            if (!tiles.empty())
+                WK_CUDA(cudaMemcpyAsync(g->d_tiles.p, tiles.data(), sizeof(uint4) * tiles.size(), cudaMemcpyHostToDevice,
+                                        g->stream));
+            if (!gen4.empty())
+                WK_CUDA(cudaMemcpyAsync(g->d_gen4.p, gen4.data(), sizeof(uint4) * gen4.size(), cudaMemcpyHostToDevice,
+                                        g->stream));
+            if (!mixed_spans.empty())
+                WK_CUDA(cudaMemcpyAsync(g->d_mixed.p, mixed_spans.data(), sizeof(uint4) * mixed_spans.size(),
+                                        cudaMemcpyHostToDevice, g->stream));
+            WK_CUDA(cudaStreamSynchronize(g->stream));  // the host vectors go out of scope
+            g->n_tiles = static_cast<int>(tiles.size());
+            g->n_tile_gen = static_cast<int>(gen4.size());
+            g->n_mixed = static_cast<int>(mixed_spans.size());
+            g->h_tiles = std::move(tiles);
+            g->h_gen4 = std::move(gen4);
+            g->h_mixed = std::move(mixed_spans);
+        }
+        g->h_fast_rows = std::move(spans);
         g->h_gen_rows = std::move(gen);
     }
     ++g->geom_version;
@@ -491,14 +558,44 @@ int do_steps(wake_grid* g, int n) {
         StepArgs a = wk::grid_step_args(g);
         a.fin = g->buf(g->cur);
         a.fout = g->buf(1 - g->cur);
+        if (g->use_tiles()) {
+            // one persistent launch for the general rows and the staged pure-gather tiles,
+            // then the momentum-exchange sum of the slots it wrote
+            const TileArgs t{g->d_tiles.as<uint4>(), g->n_tiles, g->d_gen4.as<uint4>(), g->n_tile_gen, nullptr, 0,
+                             g->d_mixed.as<uint4>(), g->n_mixed};
+            const bool timed = g->time_bulk;
+            if (timed) {
+                while (g->t_ev.size() < g->t_used + 2) {
+                    cudaEvent_t e = nullptr;
+                    WK_CUDA(cudaEventCreate(&e));
+                    g->t_ev.push_back(e);
+                }
+                WK_CUDA(cudaEventRecord(g->t_ev[g->t_used], g->stream));
+            }
+            WK_CUDA(launch_tiles_any(g->Q, g->collision, g->storage, g->les != 0, a, t, g->stream));
+            if (timed) {
+                WK_CUDA(cudaEventRecord(g->t_ev[g->t_used + 1], g->stream));
+                g->t_used += 2;
+            }
+            if (g->mem_on) {
+                k_mem_reduce<<<1, 256, 0, g->stream>>>(a.mem.contrib, a.mem.n_nodes, a.mem.hist_step, a.mem.hist,
+                                                       a.mem.hist_cap);
+                WK_CUDA(cudaGetLastError());
+            }
+            g->cur ^= 1;
+            g->mf_valid = false;
+            for (int c = 0; c < 3; ++c) g->last_step_g[c] = g->phys.g[c];
+            ++g->k;
+            continue;
+        }
         // The pure-gather rows and the rows with boundaries / momentum exchange write
         // disjoint nodes of the output, so the small general launch runs on a forked
         // stream beside the bulk launch (a fork/join that CUDA graph capture keeps).
         StepArgs gen = a;
         gen.rows = g->d_gen_rows.as<unsigned>();
         gen.nrows = g->n_gen;
-        a.rows = g->d_fast_rows.as<unsigned>();
-        a.nrows = g->n_fast;
+        a.spans = g->d_fast_rows.as<uint4>();
+        a.nspans = g->n_fast;
         const bool fork = g->n_fast > 0 && g->n_gen > 0;
         Launch side = g->launch();
         if (fork) {
@@ -513,7 +610,7 @@ int do_steps(wake_grid* g, int n) {
                                                      a.mem.hist_cap);
             WK_CUDA(cudaGetLastError());
         }
-        const bool timed = g->time_bulk && a.nrows > 0;
+        const bool timed = g->time_bulk && a.nspans > 0;
         if (timed) {
             while (g->t_ev.size() < g->t_used + 2) {
                 cudaEvent_t e = nullptr;
@@ -1133,6 +1230,7 @@ int wake_grid_synchronize(wake_grid* g) {
     WK_CUDA(cudaStreamSynchronize(g->stream));
     unsigned st = 0;
     WK_CUDA(cudaMemcpy(&st, g->d_status.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (st & ERR_STAGE_TIMEOUT) return set_error(WAKE_ERR_CUDA, "a staged tile copy did not complete (bounded wait expired)");
     if (st & ERR_NONFINITE) return set_error(WAKE_ERR_NUMERIC, "non-finite or non-positive density on the device");
     return WAKE_OK;
 }
@@ -1271,10 +1369,24 @@ int wake_grid_set_block(wake_grid* g, int threads_per_block) {
 
 int wake_grid_get_block(wake_grid* g) { return g ? g->tpb : WAKE_ERR_INVALID; }
 
+int wake_grid_set_kernel(wake_grid* g, int variant) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (variant < 0 || variant > 2) return set_error(WAKE_ERR_INVALID, "wake_grid_set_kernel: variant 0, 1 or 2");
+    g->kernel_variant = variant;
+    g->invalidate_graph();
+    return WAKE_OK;
+}
+
+int wake_grid_get_kernel(wake_grid* g) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    return g->use_tiles() ? 2 : 1;
+}
+
 int wake_grid_launches_per_step(wake_grid* g) {
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
     const int r = prepare(g);
     if (r) return r;
+    if (g->use_tiles()) return 1 + (g->mem_on ? 1 : 0);
     return (g->n_fast > 0 ? 1 : 0) + (g->n_gen > 0 ? 1 : 0) + (g->mem_on ? 1 : 0);
 }
 
@@ -1297,7 +1409,8 @@ int wake_grid_bulk_launch_times(wake_grid* g, double* total_ms, long long* launc
     }
     if (total_ms) *total_ms = sum;
     if (launches) *launches = static_cast<long long>(g->t_used / 2);
-    if (nodes_per_launch) *nodes_per_launch = static_cast<long long>(g->n_fast) * g->nx;
+    // the persistent launch also updates the general rows
+    if (nodes_per_launch) *nodes_per_launch = g->use_tiles() ? g->N : g->fast_nodes();
     g->t_used = 0;
     return WAKE_OK;
 }

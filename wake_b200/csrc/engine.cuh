@@ -38,6 +38,8 @@ struct HostLat {
 cudaError_t launch_step_any(int Q, int coll, int store, bool les, const StepArgs& a, const Launch& L, bool fast);
 cudaError_t launch_batch_any(int Q, int coll, int store, bool les, const BatchArgs& b, int tpb, cudaStream_t stream,
                              bool fast, bool idx32);
+cudaError_t launch_tiles_any(int Q, int coll, int store, bool les, const StepArgs& a, const TileArgs& t,
+                             cudaStream_t stream);
 
 }  // namespace wk
 
@@ -87,14 +89,30 @@ struct wake_grid {
     DevMem d_warp_base, d_contrib;     // momentum-exchange slots (see MemCfg)
     int warps_per_row = 1, n_mem_nodes = 0;
 
-    // rows handled by k_step_fast (pure-gather rows) and by k_step (the rest),
-    // packed (z << 16) | y
+    // pure-gather spans (0, row, x0, x1) handled by k_step_fast, and general segments
+    // (SEG nodes of a row, numbered row * nseg + s) handled by k_step
     DevMem d_fast_rows, d_gen_rows;
     int n_fast = 0, n_gen = 0;
-    std::vector<unsigned> h_fast_rows, h_gen_rows;  // host copies of the two row lists
+    std::vector<uint4> h_fast_rows;     // spans
+    std::vector<unsigned> h_gen_rows;   // general segments
+    long long fast_nodes() const {      // nodes in the pure-gather spans
+        long long n = 0;
+        for (const uint4& sp : h_fast_rows) n += sp.w - sp.z;
+        return n;
+    }
     unsigned geom_version = 0;                      // bumped whenever the flags / row lists are rebuilt
 
     int tpb = 0, xchunks = 1, rows = 1, tpb_fast = 256;
+    // step kernels: 0 automatic, 1 direct (k_step_fast for the pure-gather rows beside
+    // k_step for the rest), 2 persistent tiles (k_step_tiles: pure-gather tiles staged in
+    // shared memory plus the general rows, when the row shape allows it)
+    int kernel_variant = 0;
+    bool use_tiles() const { return kernel_variant == 2 && wk::tile_row_ok(nx, static_cast<int>(elem)); }
+    // pure-gather tiles (0, (z << 16) | y0, rows, 0) and the segments of the other rows
+    // (0, segment, general-segment entry, 0)
+    DevMem d_tiles, d_gen4, d_mixed;
+    int n_tiles = 0, n_tile_gen = 0, n_mixed = 0;
+    std::vector<uint4> h_tiles, h_gen4, h_mixed;  // h_mixed: the spans of rows outside the tiles
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaStream_t side = nullptr;  // forked stream of the general-row launch
@@ -124,7 +142,8 @@ struct wake_grid {
         if (idle) {
             DevMem* all[] = {&A, &B, &d_types, &d_flags, &d_status, &d_nodestart, &d_link_node, &d_link_q,
                              &d_link_delta, &d_link_mom, &d_counters, &d_hist, &d_warp_base, &d_contrib,
-                             &d_fast_rows, &d_gen_rows, &m_f, &m_rho, &m_ux, &m_uy, &m_uz, &m_speed, &m_diag};
+                             &d_fast_rows, &d_gen_rows, &d_tiles, &d_gen4, &d_mixed, &m_f, &m_rho, &m_ux, &m_uy, &m_uz,
+                             &m_speed, &m_diag};
             for (DevMem* m : all) m->release();
         }
         for (cudaEvent_t e : t_ev) cudaEventDestroy(e);

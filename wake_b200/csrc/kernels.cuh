@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include "staged.cuh"
 #include "stream_collide.cuh"
 
 namespace wk {
@@ -14,7 +15,7 @@ struct Launch {
     int rows;      // ny * nz
     cudaStream_t stream;
     int ny, nz;
-    int tpb_fast;  // threads per block of k_step_fast (<= 256)
+    int tpb_fast;  // threads per block of k_step_fast (<= 256; one warp per segment)
 };
 
 struct FlagCfg {
@@ -30,6 +31,8 @@ struct FlagCfg {
     cudaError_t launch_step_q##Q(int coll, int store, bool les, const StepArgs& a, const Launch& L, bool fast);  \
     cudaError_t launch_batch_q##Q(int coll, int store, bool les, const BatchArgs& b, int tpb,                   \
                                   cudaStream_t stream, bool fast, bool idx32);                                  \
+    cudaError_t launch_tiles_q##Q(int coll, int store, bool les, const StepArgs& a, const TileArgs& t,          \
+                                  cudaStream_t stream);                                                          \
     cudaError_t launch_materialise_q##Q(int store, const void* fin, const uint8_t* flags, const Geo& geo,        \
                                         const Links& links, const Physics& phys, const Out& out,                 \
                                         const Launch& L, int direct);                                            \
@@ -37,7 +40,8 @@ struct FlagCfg {
                                     const uint8_t* flags, const Geo& geo, const Physics& phys, const Launch& L); \
     cudaError_t launch_flags_q##Q(const uint8_t* types, uint8_t* flags, const Geo& geo, const FlagCfg& cfg,      \
                                   const Launch& L);                                                              \
-    cudaError_t launch_row_class_q##Q(const uint8_t* flags, uint8_t* cls, const Geo& geo, const Launch& L);
+    cudaError_t launch_seg_class_q##Q(const uint8_t* flags, uint8_t* cls, const Geo& geo, long long nsegs,       \
+                                      cudaStream_t stream);
 
 WK_DECLARE_LAUNCHERS(9)
 WK_DECLARE_LAUNCHERS(19)

@@ -76,20 +76,25 @@ __global__ void k_flags(const uint8_t* __restrict__ types, uint8_t* __restrict__
     flags[i] = fl;
 }
 
-// Row classes for the two step kernels: bit 0 = every node of the row is a pure
-// gather (k_step_fast), bit 1 = the row holds a momentum-exchange node.
+// Segment classes for the two step kernels (one warp per segment of SEG nodes):
+// bit 0 = every node is a pure gather (k_step_fast), bit 1 = the segment holds
+// a momentum-exchange node.
 template <int Q>
-__global__ void k_row_class(const uint8_t* __restrict__ flags, uint8_t* __restrict__ cls, const Geo geo) {
-    const long long row0 = static_cast<long long>(blockIdx.x) * geo.nx;
-    int all_fast = 1, any_mem = 0;
-    for (int x = threadIdx.x; x < geo.nx; x += blockDim.x) {
-        const uint8_t fl = flags[row0 + x];
-        all_fast &= (fl & FL_FAST) ? 1 : 0;
-        any_mem |= (fl & FL_MEM) ? 1 : 0;
+__global__ void k_seg_class(const uint8_t* __restrict__ flags, uint8_t* __restrict__ cls, const Geo geo,
+                            long long nsegs) {
+    const long long e = blockIdx.x * static_cast<long long>(blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (e >= nsegs) return;
+    const Seg sg = seg_decode(static_cast<unsigned>(e), geo);
+    const int lane = threadIdx.x & 31;
+    int fast = 1, mem = 0;
+    for (int x = sg.x0 + lane; x < sg.x1; x += 32) {
+        const uint8_t fl = flags[sg.row0 + x];
+        fast &= (fl & FL_FAST) ? 1 : 0;
+        mem |= (fl & FL_MEM) ? 1 : 0;
     }
-    all_fast = __syncthreads_and(all_fast);
-    any_mem = __syncthreads_or(any_mem);
-    if (threadIdx.x == 0) cls[blockIdx.x] = static_cast<uint8_t>((all_fast ? 1 : 0) | (any_mem ? 2 : 0));
+    fast = __all_sync(0xffffffffu, fast);
+    mem = __any_sync(0xffffffffu, mem);
+    if (lane == 0) cls[e] = static_cast<uint8_t>((fast ? 1 : 0) | (mem ? 2 : 0));
 }
 
 // Pull-free read of f^0 (state buffer holding pre-collision populations).
@@ -127,14 +132,15 @@ constexpr int kQ = WK_Q;
 
 template <int C, int S, bool LES>
 void step_one(const StepArgs& a, const Launch& L, bool fast) {
-    if (a.nrows <= 0) return;
     if (fast) {
-        // 32-bit element indexing whenever every index of the state buffer fits
+        if (a.nspans <= 0) return;
+        // one block per span; 32-bit element indexing whenever every index of the state buffer fits
         const bool idx32 = static_cast<long long>(kQ) * a.geo.pitch < (1ll << 32);
-        if (idx32) k_step_fast<kQ, C, S, LES, true><<<a.nrows, L.tpb_fast, 0, L.stream>>>(a);
-        else k_step_fast<kQ, C, S, LES, false><<<a.nrows, L.tpb_fast, 0, L.stream>>>(a);
+        if (idx32) k_step_fast<kQ, C, S, LES, true><<<a.nspans, L.tpb_fast, 0, L.stream>>>(a);
+        else k_step_fast<kQ, C, S, LES, false><<<a.nspans, L.tpb_fast, 0, L.stream>>>(a);
     } else {
-        k_step<kQ, C, S, LES><<<a.nrows, L.tpb, 0, L.stream>>>(a);
+        if (a.nrows <= 0) return;
+        k_step<kQ, C, S, LES><<<a.nrows, 64, 0, L.stream>>>(a);
     }
 }
 template <int C, int S, bool LES>
@@ -144,14 +150,43 @@ void initial_one(const float* f0, void* A, void* B, const uint8_t* flags, const 
 }
 template <int C, int S, bool LES>
 void batch_one(const BatchArgs& b, int tpb, cudaStream_t st, bool fast, bool idx32) {
-    if (b.nrows <= 0) return;
     if (fast) {
-        if (idx32) k_step_fast_batch<kQ, C, S, LES, true><<<b.nrows, tpb, 0, st>>>(b);
-        else k_step_fast_batch<kQ, C, S, LES, false><<<b.nrows, tpb, 0, st>>>(b);
+        if (b.nspans <= 0) return;
+        if (idx32) k_step_fast_batch<kQ, C, S, LES, true><<<b.nspans, tpb, 0, st>>>(b);
+        else k_step_fast_batch<kQ, C, S, LES, false><<<b.nspans, tpb, 0, st>>>(b);
     } else {
-        k_step_batch<kQ, C, S, LES><<<b.nrows, tpb, 0, st>>>(b);
+        if (b.nrows <= 0) return;
+        k_step_batch<kQ, C, S, LES><<<b.nrows, 64, 0, st>>>(b);
     }
 }
+// Persistent tile kernel: TILE_CTAS_PER_SM CTAs per SM (capped by the work), dynamic shared
+// memory opted in once per kernel instantiation.
+template <auto Kernel>
+cudaError_t tiles_launch(unsigned smem, int work, cudaStream_t st, const StepArgs& a, const TileArgs& t) {
+    static bool ready = false;
+    if (!ready) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        ready = true;
+    }
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int blocks = std::max(1, std::min(work, TILE_CTAS_PER_SM * sms));
+    Kernel<<<blocks, TILE_THREADS, smem, st>>>(a, t);
+    return cudaGetLastError();
+}
+
+template <int C, int S, bool LES>
+cudaError_t tiles_one(const StepArgs& a, const TileArgs& t, cudaStream_t st) {
+    constexpr unsigned smem = tile_smem_bytes<kQ, S>();
+    const int work = std::max(std::max(t.ntiles, t.ngen), t.nspans);
+    if (work <= 0) return cudaSuccess;
+    if (t.dom) return tiles_launch<k_step_tiles<kQ, C, S, LES, true>>(smem, work, st, a, t);
+    return tiles_launch<k_step_tiles<kQ, C, S, LES, false>>(smem, work, st, a, t);
+}
+using TilesFn = cudaError_t (*)(const StepArgs&, const TileArgs&, cudaStream_t);
 using StepFn = void (*)(const StepArgs&, const Launch&, bool);
 using BatchFn = void (*)(const BatchArgs&, int, cudaStream_t, bool, bool);
 using InitFn = void (*)(const float*, void*, void*, const uint8_t*, const Geo&, const Physics&, const Launch&);
@@ -168,9 +203,14 @@ const InitFn kInit[3][3][2] = {{WK_IROW(0, 0), WK_IROW(0, 1), WK_IROW(0, 2)},
 const BatchFn kBatch[3][3][2] = {{WK_BROW(0, 0), WK_BROW(0, 1), WK_BROW(0, 2)},
                                  {WK_BROW(1, 0), WK_BROW(1, 1), WK_BROW(1, 2)},
                                  {WK_BROW(2, 0), WK_BROW(2, 1), WK_BROW(2, 2)}};
+#define WK_SROW(C, S) {tiles_one<C, S, false>, tiles_one<C, S, true>}
+const TilesFn kTiles[3][3][2] = {{WK_SROW(0, 0), WK_SROW(0, 1), WK_SROW(0, 2)},
+                                 {WK_SROW(1, 0), WK_SROW(1, 1), WK_SROW(1, 2)},
+                                 {WK_SROW(2, 0), WK_SROW(2, 1), WK_SROW(2, 2)}};
 #undef WK_ROW
 #undef WK_IROW
 #undef WK_BROW
+#undef WK_SROW
 
 bool valid(int coll, int store) { return coll >= 0 && coll < 3 && store >= 0 && store < 3; }
 }  // namespace
@@ -187,6 +227,12 @@ cudaError_t WK_CAT(launch_batch_q, WK_Q)(int coll, int store, bool les, const Ba
     if (!valid(coll, store)) return cudaErrorInvalidValue;
     kBatch[coll][store][les ? 1 : 0](b, tpb, stream, fast, idx32);
     return cudaGetLastError();
+}
+
+cudaError_t WK_CAT(launch_tiles_q, WK_Q)(int coll, int store, bool les, const StepArgs& a, const TileArgs& t,
+                                        cudaStream_t stream) {
+    if (!valid(coll, store)) return cudaErrorInvalidValue;
+    return kTiles[coll][store][les ? 1 : 0](a, t, stream);
 }
 
 cudaError_t WK_CAT(launch_initial_q, WK_Q)(int coll, int store, bool les, const float* f0, void* a, void* b,
@@ -225,8 +271,11 @@ cudaError_t WK_CAT(launch_flags_q, WK_Q)(const uint8_t* types, uint8_t* flags, c
     return cudaGetLastError();
 }
 
-cudaError_t WK_CAT(launch_row_class_q, WK_Q)(const uint8_t* flags, uint8_t* cls, const Geo& geo, const Launch& L) {
-    k_row_class<kQ><<<L.rows, 256, 0, L.stream>>>(flags, cls, geo);
+cudaError_t WK_CAT(launch_seg_class_q, WK_Q)(const uint8_t* flags, uint8_t* cls, const Geo& geo, long long nsegs,
+                                            cudaStream_t stream) {
+    if (nsegs <= 0) return cudaSuccess;
+    const long long blocks = (nsegs + 7) / 8;
+    k_seg_class<kQ><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(flags, cls, geo, nsegs);
     return cudaGetLastError();
 }
 

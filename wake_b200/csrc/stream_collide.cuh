@@ -16,6 +16,7 @@
 #pragma once
 
 #include "lattice.cuh"
+#include "pairs2.cuh"
 
 namespace wk {
 
@@ -45,11 +46,12 @@ struct MemCfg {                   // momentum-exchange monitor
     float center[3];
     float r_max, r_max_sq;
     // Every node carrying FL_MEM owns one fixed slot of `contrib`, numbered in node
-    // order: slot = warp_base[entry * warps_per_row + x / 32] + (rank of the node
-    // among the FL_MEM nodes of its 32-wide chunk). k_mem_reduce sums the slots in
-    // slot order, so the force is reproducible bit for bit and needs no barrier.
-    const int* warp_base;         // [general rows][warps_per_row]
-    int warps_per_row;
+    // order: slot = warp_base[entry * warps_per_row + chunk] + (rank of the node
+    // among the FL_MEM nodes of its 32-node chunk of a general segment). k_mem_reduce
+    // sums the slots in slot order, so the force is reproducible bit for bit and
+    // needs no barrier.
+    const int* warp_base;         // [general segments][warps_per_row]
+    int warps_per_row;            // 32-node chunks per segment (SEG / 32)
     double* contrib;              // [n_nodes][3]
     int n_nodes;
     unsigned* hist_step;          // number of entries written so far
@@ -216,37 +218,77 @@ struct StepArgs {
     Links links;
     MemCfg mem;
     Physics phys;
-    const unsigned* rows;  // rows of this launch, packed (z << 16) | y; one block per row
+    const unsigned* rows;  // general segments of this launch (seg_decode); one block per segment
     int nrows;
+    const uint4* spans;    // pure-gather spans (member, row, x0, x1); one block per span
+    int nspans;
 };
 
-// One fused time step of one row: g^{k+1} = Collide(ZouHe(BFL(Pull(g^k)))). Solid
-// nodes are not touched: both buffers hold their frozen populations. `e` is the row
-// (z << 16) | y, `entry` its index in the launch's general-row list (momentum-exchange
-// slots are numbered per entry).
+// Work unit of the step kernels: a segment of up to SEG consecutive nodes of one
+// row, numbered row * nseg + s with nseg = ceil(nx / SEG) and row = z * ny + y.
+// Rows are split so that only the segments next to a wall, obstacle or curved
+// link take the general per-node path.
+constexpr int SEG = 64;
+
+struct Seg {
+    int y, z, x0, x1;
+    long long row0;  // index of node (0, y, z)
+};
+
+__device__ __forceinline__ Seg seg_decode(unsigned e, const Geo& g) {
+    const unsigned nseg = static_cast<unsigned>((g.nx + SEG - 1) / SEG);
+    const unsigned row = e / nseg;
+    Seg s;
+    s.x0 = static_cast<int>(e - row * nseg) * SEG;
+    s.x1 = min(g.nx, s.x0 + SEG);
+    s.y = static_cast<int>(row % static_cast<unsigned>(g.ny));
+    s.z = static_cast<int>(row / static_cast<unsigned>(g.ny));
+    s.row0 = static_cast<long long>(row) * g.nx;
+    return s;
+}
+
+// A span: nodes x0 .. x1-1 of one row, all pure gathers (a whole row, or a run of
+// pure-gather segments of a row that also holds general segments).
+__device__ __forceinline__ Seg span_decode(uint4 sp, const Geo& g) {
+    Seg s;
+    s.y = static_cast<int>(sp.y % static_cast<unsigned>(g.ny));
+    s.z = static_cast<int>(sp.y / static_cast<unsigned>(g.ny));
+    s.x0 = static_cast<int>(sp.z);
+    s.x1 = static_cast<int>(sp.w);
+    s.row0 = static_cast<long long>(sp.y) * g.nx;
+    return s;
+}
+
+// One fused time step of one 32-node chunk (0 or 1) of segment e, by one warp:
+// g^{k+1} = Collide(ZouHe(BFL(Pull(g^k)))). Solid nodes are not touched: both
+// buffers hold their frozen populations. `entry` is the segment's index in its
+// lattice's general-segment list; momentum-exchange slots are numbered per
+// (entry, chunk).
 template <int Q, int COLL, int S, bool LES>
-__device__ __forceinline__ void step_row(const StepArgs& a, unsigned e, int entry) {
+__device__ __forceinline__ void step_chunk(const StepArgs& a, unsigned e, int entry, int chunk) {
     using L = Lat<Q>;
     using C = Codec<S>;
     using T = typename C::T;
-    const int y = static_cast<int>(e & 0xffffu), z = static_cast<int>(e >> 16);
-    const long long row0 = (static_cast<long long>(z) * a.geo.ny + y) * a.geo.nx;
-    const int nx = a.geo.nx, lane = threadIdx.x & 31;
-    // warps walk the row in 32-wide chunks (x = chunk + lane)
-    for (int xb = threadIdx.x - lane; xb < nx; xb += blockDim.x) {
+    const Seg sg = seg_decode(e, a.geo);
+    const int y = sg.y, z = sg.z;
+    const long long row0 = sg.row0;
+    const int lane = threadIdx.x & 31;
+    const int xb = sg.x0 + 32 * chunk;
+    if (xb >= sg.x1) return;
+    {
         const int x = xb + lane;
-        if (x >= nx) continue;
-        const long long i = row0 + x;
+        const bool live_node = x < sg.x1;
+        const long long i = row0 + (live_node ? x : xb);
         const uint8_t fl = a.flags[i];
         int slot = -1;
         if (a.mem.enabled) {
             // slot = chunk base + rank among this chunk's momentum-exchange nodes
-            const unsigned live = (nx - xb >= 32) ? 0xffffffffu : ((1u << (nx - xb)) - 1u);
-            const bool m = (fl & FL_MEM) != 0;
-            const unsigned bal = __ballot_sync(live, m);
-            if (m) slot = a.mem.warp_base[entry * a.mem.warps_per_row + (xb >> 5)] + __popc(bal & ((1u << lane) - 1u));
+            const bool m = live_node && (fl & FL_MEM) != 0;
+            const unsigned bal = __ballot_sync(0xffffffffu, m);
+            if (m) slot = a.mem.warp_base[entry * a.mem.warps_per_row + chunk] + __popc(bal & ((1u << lane) - 1u));
         }
-        if ((fl & FL_TYPE) == CT_SOLID) continue;
+        if (!live_node) return;
+        if ((fl & FL_TYPE) == CT_SOLID) return;
         float f[Q];
         unsigned bb;
         gather<Q, S>(static_cast<const T*>(a.fin), a.geo, a.flags, a.links, x, y, z, i, fl, f, bb);
@@ -268,19 +310,124 @@ __device__ __forceinline__ void step_row(const StepArgs& a, unsigned e, int entr
     }
 }
 
+// Value stored for population q: FP32 holds f, FP16 / BF16 hold h = f / w - 1.
+// load_h / store_h move the stored value itself (no decode) for the h-space math.
+template <int S>
+__device__ __forceinline__ float load_raw(const typename Codec<S>::T* p) {
+    if constexpr (S == STORE_F32) return __ldg(p);
+    else if constexpr (S == STORE_F16) return __half2float(__ldg(p));
+    else return __bfloat162float(__ldg(p));
+}
+template <int S>
+__device__ __forceinline__ void store_raw(typename Codec<S>::T* p, float v) {
+    if constexpr (S == STORE_F32) __stcs(p, v);
+    else if constexpr (S == STORE_F16) __stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(__float2half_rn(v)));
+    else __stcs(reinterpret_cast<unsigned short*>(p), __bfloat16_as_ushort(__float2bfloat16_rn(v)));
+}
+
+// Zou-He on one of the two nodes of a packed pair (lane 0 = .x, 1 = .y); the
+// formulas work on f, so shifted values are decoded and encoded around them.
+template <int Q, bool HS>
+__device__ __forceinline__ void zou_he_half(float2* f, int lane, uint8_t fl, const Geo& G) {
+    using L = Lat<Q>;
+    float t[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const float v = lane ? f[q].y : f[q].x;
+        t[q] = HS ? fmaf(L::w(q), v, L::w(q)) : v;
+    }
+    if (fl & FL_ZH_IN) zou_he_inlet<Q>(t, G.uin);
+    if (fl & FL_ZH_OUT) zou_he_outlet<Q>(t, G.rho_out);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const float v = HS ? fmaf(t[q], 1.0f / L::w(q), -1.0f) : t[q];
+        if (lane) f[q].y = v;
+        else f[q].x = v;
+    }
+}
+
+// TRT pure-gather span, one block: each warp takes 64-node chunks, two nodes per
+// thread (base + lane and base + lane + 32) in packed FP32 (trt_pairs2); shifted
+// storage is updated in h directly.
+template <int Q, int S, bool LES, bool IDX32>
+__device__ __forceinline__ void step_span_fast2(const StepArgs& a, const Seg& sg) {
+    using L = Lat<Q>;
+    using C = Codec<S>;
+    using T = typename C::T;
+    constexpr bool HS = S != STORE_F32;
+    const int nx = a.geo.nx, ny = a.geo.ny, nz = a.geo.nz;
+    const int y = sg.y, z = sg.z;
+    const long long row0 = sg.row0;
+    const int yl = (y + 1 == ny) ? (a.geo.periodic_y ? 0 : y + 1) : y + 1;
+    const int yh = (y == 0) ? (a.geo.periodic_y ? ny - 1 : -1) : y - 1;
+    const int zl = (z + 1 == nz) ? (a.geo.periodic_z ? 0 : z + 1) : z + 1;
+    const int zh = (z == 0) ? (a.geo.periodic_z ? nz - 1 : -1) : z - 1;
+    const int ysrc[3] = {yl, y, yh}, zsrc[3] = {zl, z, zh};
+    const T* fin = static_cast<const T*>(a.fin);
+    T* out = static_cast<T*>(a.fout);
+    const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (int base = sg.x0 + (threadIdx.x >> 5) * 64; base < sg.x1; base += nwarps * 64) {
+        const int xa = base + lane;
+        if (xa >= sg.x1) continue;
+        const bool vb = xa + 32 < sg.x1;
+        const int xb = vb ? xa + 32 : xa;  // a short chunk computes node a twice and stores it once
+        const uint8_t fa = a.flags[row0 + xa], fb = a.flags[row0 + xb];
+        const int xsa[3] = {xa + 1 == nx ? 0 : xa + 1, xa, xa == 0 ? nx - 1 : xa - 1};
+        const int xsb[3] = {xb + 1 == nx ? 0 : xb + 1, xb, xb == 0 ? nx - 1 : xb - 1};
+        float2 f[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            if constexpr (IDX32) {
+                const unsigned P = static_cast<unsigned>(a.geo.pitch);
+                const unsigned rowsrc = static_cast<unsigned>((zsrc[L::cz(q) + 1] * ny + ysrc[L::cy(q) + 1]) * nx);
+                const T* pl = fin + (q * P + rowsrc);
+                f[q] = make_float2(load_raw<S>(pl + xsa[L::cx(q) + 1]), load_raw<S>(pl + xsb[L::cx(q) + 1]));
+            } else {
+                const long long rowsrc = (static_cast<long long>(zsrc[L::cz(q) + 1]) * ny + ysrc[L::cy(q) + 1]) * nx;
+                const T* pl = fin + (q * a.geo.pitch + rowsrc);
+                f[q] = make_float2(load_raw<S>(pl + xsa[L::cx(q) + 1]), load_raw<S>(pl + xsb[L::cx(q) + 1]));
+            }
+        }
+        if ((fa | fb) & (FL_ZH_IN | FL_ZH_OUT)) {
+            if (fa & (FL_ZH_IN | FL_ZH_OUT)) zou_he_half<Q, HS>(f, 0, fa, a.geo);
+            if (fb & (FL_ZH_IN | FL_ZH_OUT)) zou_he_half<Q, HS>(f, 1, fb, a.geo);
+        }
+        float2 rho, u[3];
+        trt_pairs2<Q, LES, HS>(f, a.phys, rho, u);
+        const bool bad = !(rho.x > 0.0f) || !(fabsf(u[0].x) < 1e30f) || (vb && (!(rho.y > 0.0f) || !(fabsf(u[0].y) < 1e30f)));
+        if (bad) atomicOr(a.status, ERR_NONFINITE);
+        T* oa = out + (row0 + xa);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            if constexpr (IDX32) {
+                const unsigned P = static_cast<unsigned>(a.geo.pitch);
+                store_raw<S>(oa + q * P, f[q].x);
+                if (vb) store_raw<S>(oa + (q * P + 32u), f[q].y);
+            } else {
+                store_raw<S>(oa + q * a.geo.pitch, f[q].x);
+                if (vb) store_raw<S>(oa + (q * a.geo.pitch + 32), f[q].y);
+            }
+        }
+    }
+}
+
 // The same step for a row whose every node is a pure gather (no solid, no
 // bounce-back, no curved link; Zou-He allowed) -- the bulk of a domain. Without
 // the rare paths the kernel fits 64 registers.
 template <int Q, int COLL, int S, bool LES, bool IDX32>
-__device__ __forceinline__ void step_row_fast(const StepArgs& a, unsigned e) {
+__device__ __forceinline__ void step_span_fast(const StepArgs& a, const Seg& sg) {
+    if constexpr (COLL == COLL_TRT) {
+        step_span_fast2<Q, S, LES, IDX32>(a, sg);
+        return;
+    }
     using L = Lat<Q>;
     using C = Codec<S>;
     using T = typename C::T;
     const int nx = a.geo.nx, ny = a.geo.ny, nz = a.geo.nz;
-    const int y = static_cast<int>(e & 0xffffu), z = static_cast<int>(e >> 16);
-    const long long row0 = (static_cast<long long>(z) * ny + y) * nx;
+    const int y = sg.y, z = sg.z;
+    const long long row0 = sg.row0;
     // Source-row offsets of the (cy, cz) shifts relative to this row, y / z wraps
-    // applied: uniform across the block, so with the plane offsets they form
+    // applied: uniform across the warp, so with the plane offsets they form
     // warp-uniform address terms and each load is a per-thread base plus a uniform offset.
     const int yl = (y + 1 == ny) ? (a.geo.periodic_y ? 0 : y + 1) : y + 1;  // source row for cy = -1
     const int yh = (y == 0) ? (a.geo.periodic_y ? ny - 1 : -1) : y - 1;     // source row for cy = +1
@@ -289,7 +436,7 @@ __device__ __forceinline__ void step_row_fast(const StepArgs& a, unsigned e) {
     const int ysrc[3] = {yl, y, yh}, zsrc[3] = {zl, z, zh};
     const T* fin = static_cast<const T*>(a.fin);
     T* out = static_cast<T*>(a.fout);
-    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+    for (int x = sg.x0 + threadIdx.x; x < sg.x1; x += blockDim.x) {
         const uint8_t fl = a.flags[row0 + x];
         // source x for cx = -1, 0, +1 (periodic in x)
         const int xs[3] = {x + 1 == nx ? 0 : x + 1, x, x == 0 ? nx - 1 : x - 1};
@@ -333,15 +480,17 @@ __device__ __forceinline__ void step_row_fast(const StepArgs& a, unsigned e) {
     }
 }
 
-// Single lattice: one block per listed row.
+// Single lattice. General segments: one 64-thread block per segment (a warp per
+// 32-node chunk). Pure-gather spans: one block per span.
 template <int Q, int COLL, int S, bool LES>
-__global__ void __launch_bounds__(512) k_step(const StepArgs a) {
-    step_row<Q, COLL, S, LES>(a, a.rows[blockIdx.x], blockIdx.x);
+__global__ void __launch_bounds__(64) k_step(const StepArgs a) {
+    step_chunk<Q, COLL, S, LES>(a, a.rows[blockIdx.x], blockIdx.x, threadIdx.x >> 5);
 }
 
+// TRT segments carry two nodes per thread (twice the registers, half the threads per node).
 template <int Q, int COLL, int S, bool LES, bool IDX32>
-__global__ void __launch_bounds__(256, 4) k_step_fast(const StepArgs a) {
-    step_row_fast<Q, COLL, S, LES, IDX32>(a, a.rows[blockIdx.x]);
+__global__ void __launch_bounds__(256, COLL == COLL_TRT ? 2 : 4) k_step_fast(const StepArgs a) {
+    step_span_fast<Q, COLL, S, LES, IDX32>(a, span_decode(a.spans[blockIdx.x], a.geo));
 }
 
 // ------------------------------------------------------------------ many lattices
@@ -358,9 +507,11 @@ struct BatchDom {
 
 struct BatchArgs {
     const BatchDom* dom;
-    const uint2* rows;   // (member, (z << 16) | y), one block per entry
+    const uint2* rows;   // general segments (member, segment), one block per entry
     int nrows;
     int parity;          // batch step parity of this launch
+    const uint4* spans;  // pure-gather spans (member, row, x0, x1), one block per entry
+    int nspans;
 };
 
 __device__ __forceinline__ StepArgs batch_member(const BatchArgs& b, unsigned m) {
@@ -373,17 +524,17 @@ __device__ __forceinline__ StepArgs batch_member(const BatchArgs& b, unsigned m)
 }
 
 template <int Q, int COLL, int S, bool LES>
-__global__ void __launch_bounds__(512) k_step_batch(const BatchArgs b) {
+__global__ void __launch_bounds__(64) k_step_batch(const BatchArgs b) {
     const uint2 r = b.rows[blockIdx.x];
     const StepArgs a = batch_member(b, r.x);
-    step_row<Q, COLL, S, LES>(a, r.y, static_cast<int>(blockIdx.x) - b.dom[r.x].gen_first);
+    step_chunk<Q, COLL, S, LES>(a, r.y, static_cast<int>(blockIdx.x) - b.dom[r.x].gen_first, threadIdx.x >> 5);
 }
 
 template <int Q, int COLL, int S, bool LES, bool IDX32>
-__global__ void __launch_bounds__(256, 4) k_step_fast_batch(const BatchArgs b) {
-    const uint2 r = b.rows[blockIdx.x];
-    const StepArgs a = batch_member(b, r.x);
-    step_row_fast<Q, COLL, S, LES, IDX32>(a, r.y);
+__global__ void __launch_bounds__(256, COLL == COLL_TRT ? 2 : 4) k_step_fast_batch(const BatchArgs b) {
+    const uint4 sp = b.spans[blockIdx.x];
+    const StepArgs a = batch_member(b, sp.x);
+    step_span_fast<Q, COLL, S, LES, IDX32>(a, span_decode(sp, a.geo));
 }
 
 // Sum one step's momentum-exchange slots in slot order with one 256-thread block
