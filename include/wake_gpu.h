@@ -287,6 +287,24 @@ int wake_grid_launches_per_step(wake_grid* g);
 int wake_grid_time_bulk_launches(wake_grid* g, int on);
 int wake_grid_bulk_launch_times(wake_grid* g, double* total_ms, long long* launches, long long* nodes_per_launch);
 
+/* Coupled temperature (D2Q9 lattices only; no reference counterpart: the
+ * reference's ThermalSolver2D, src/thermal/thermal_solver.cpp:83-123, carries a
+ * D2Q9 temperature and drives the flow with one domain-averaged force,
+ * src/scenarios/thermal_convection.cpp:70). A D2Q5 temperature lattice advances
+ * in the same fused step as the flow: per node T = sum g, the flow collides
+ * with the body force (gx, gy + beta_g (T - t_ref)) (local Boussinesq), the
+ * temperature relaxes with tau_t to w_q T (1 + 3 c_q.u). The y walls hold
+ * t_south (y = -1/2) and t_north (y = ny - 1/2) by anti-bounce-back; solid
+ * nodes are adiabatic. enable before the first step (the temperature starts at
+ * t_ref); initialize_temperature sets a per-node start (host or device array of
+ * N floats) and restarts the coupled run at step 0 from the flow's initial
+ * state. The collision model, tau and body force are fixed once the grid has
+ * stepped. get_temperature returns the temperature of the last step (N floats).
+ * Thermal grids run every node on the general per-node path. */
+int wake_grid_enable_thermal(wake_grid* g, float tau_t, float t_ref, float beta_g, float t_south, float t_north);
+int wake_grid_initialize_temperature(wake_grid* g, const float* T);
+int wake_grid_get_temperature(wake_grid* g, float* T);
+
 /* Rotated solid ellipse, semi-axes a (along the rotated x axis) and b, angle in
  * radians; extruded along z in 3D. Cell-centre test in float like
  * GeometryPrimitives::voxelize_ellipsoid (src/geometry/primitives.cpp:73-99),
@@ -294,8 +312,8 @@ int wake_grid_bulk_launch_times(wake_grid* g, double* total_ms, long long* launc
 int wake_grid_set_solid_ellipse(wake_grid* g, float cx, float cy, float a, float b, float angle);
 
 /* Device memory: what the grid holds now, and an upper estimate for a new grid
- * of that shape (state buffers, FP32 initialisation scratch, flags, tables and,
- * with with_fields, the macroscopic-field scratch). release_scratch first
+ * of that shape (state buffers, FP32 initialisation scratch, flags, tables;
+ * with_fields bit 0 adds the macroscopic-field scratch, bit 1 a coupled temperature). release_scratch first
  * completes any pending setup (flags, initial collide), then frees the FP32
  * population and field scratch (re-allocated on demand by the readers). A
  * parameter change after it and before the first step re-collides f^0 as held

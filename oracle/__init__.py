@@ -51,6 +51,8 @@ class Params(C.Structure):
         ("tau", C.c_double), ("tau_bulk", C.c_double), ("lambda_trt", C.c_double), ("cs_smag", C.c_double),
         ("g", C.c_double * 3), ("u_in", C.c_double * 3), ("rho_out", C.c_double), ("u_wall", C.c_double * 3),
         ("center", C.c_double * 3), ("r_max", C.c_double), ("s3", C.c_double), ("s4", C.c_double),
+        ("thermal", C.c_int), ("tau_t", C.c_double), ("t_ref", C.c_double), ("beta_g", C.c_double),
+        ("t_south", C.c_double), ("t_north", C.c_double),
     ]
 
 
@@ -75,6 +77,7 @@ def lib() -> C.CDLL:
             "og_collide_nodes": (None, [vp, C.c_longlong, vp, vp, vp, vp, vp, vp, vp]),
             "og_d3q19_minv": (D, [I, I, I]), "og_strouhal_frequency": (D, [vp, I, D]),
             "og_smagorinsky_tau": (D, [I, vp, D, D, D, D, D, D]),
+            "og_set_thermal_state": (None, [vp, vp]), "og_get_temperature": (None, [vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -169,6 +172,16 @@ class OracleGrid:
         uy = np.ascontiguousarray(uy if uy is not None else z, np.float64)
         uz = np.ascontiguousarray(uz if uz is not None else z, np.float64)
         lib().og_set_state(self._h, _addr(f), _addr(rho), _addr(ux), _addr(uy), _addr(uz))
+
+    def set_thermal_state(self, t5):
+        """D2Q5 temperature populations [5][n] (D2Q9 grids configured with thermal=1)."""
+        t5 = np.ascontiguousarray(t5, np.float64).reshape(5, self.n)
+        lib().og_set_thermal_state(self._h, _addr(t5))
+
+    def temperature(self):
+        out = np.empty(self.n)
+        lib().og_get_temperature(self._h, _addr(out))
+        return out
 
     def set_links(self, idx, q, delta, uw=None):
         idx = np.ascontiguousarray(idx, np.int32)

@@ -32,7 +32,15 @@
 //   * y/z periodic wrap together with solids in 3D,
 //   * D3Q27 raw-moment MRT on the tensor-product monomial basis
 //     (d'Humieres et al. 2002; Geier et al. 2015 factorisation),
-//   * exact (unrounded) D3Q19 MRT inverse M^T diag(1/|M_k|^2).
+//   * exact (unrounded) D3Q19 MRT inverse M^T diag(1/|M_k|^2),
+//   * D2Q5 temperature coupled to the D2Q9 flow with a local Boussinesq force
+//     (the reference couples a D2Q9 temperature through one domain-averaged
+//     force, src/scenarios/thermal_convection.cpp:70): per node
+//       T = sum g,  a_y = beta_g (T - T_ref) added to the body force of the
+//       flow collision, g_q* = g_q - (g_q - w_q T (1 + 3 c_q.u)) / tau_T with u
+//       the flow's forced velocity (first-order equilibrium as thermal_kernels.ispc:32),
+//     streaming with anti-bounce-back g_q = -g*_opp + 2 w_q T_wall through the
+//     y walls (Dirichlet; Ginzburg 2005) and bounce-back at solid nodes (adiabatic).
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -444,6 +452,16 @@ inline void zou_he_out_d3q19(R* f, R rho) {
     f[12] = f[13] - rho * ux / R(6) - Nz;
 }
 
+// D2Q5 temperature lattice: rest, +x, +y, -x, -y (the first five D2Q9 directions), c_s^2 = 1/3.
+struct D2Q5T {
+    static constexpr int Q = 5;
+    static constexpr int cx[5] = {0, 1, 0, -1, 0};
+    static constexpr int cy[5] = {0, 0, 1, 0, -1};
+    static constexpr int opp[5] = {0, 3, 4, 1, 2};
+    static constexpr double wn[5] = {2, 1, 1, 1, 1};  // w = wn / 6
+    static constexpr double wd = 6.0;
+};
+
 // ----------------------------------------------------------------------------- grid oracle
 struct Params {
     int collision;      // 0 BGK, 1 TRT, 2 MRT
@@ -462,6 +480,8 @@ struct Params {
     double center[3];
     double r_max;
     double s3, s4;      // D3Q27 MRT higher-order rates
+    int thermal;        // D2Q9 only: D2Q5 temperature with local Boussinesq force
+    double tau_t, t_ref, beta_g, t_south, t_north;
 };
 
 template <class L, class R>
@@ -473,9 +493,12 @@ struct Grid {
     std::vector<uint8_t> type;
     std::vector<int> link_idx, link_q;
     std::vector<R> link_delta, link_uw;
+    std::vector<R> tsrc, tdst;  // D2Q5 temperature populations [5][n] (thermal only)
     Params p{};
 
     Grid(int nx_, int ny_, int nz_) : nx(nx_), ny(ny_), nz(nz_), n(std::size_t(nx_) * ny_ * nz_) {
+        tsrc.assign(5 * n, R(0));
+        tdst.assign(5 * n, R(0));
         fsrc.assign(L::Q * n, R(0));
         fdst.assign(L::Q * n, R(0));
         rho.assign(n, R(1));
@@ -503,8 +526,8 @@ struct Grid {
         return smagorinsky_tau<L, R>(f, r, u, R(p.tau), R(p.cs_smag));
     }
 
-    void collide_node(const R* f, R* out, R& r, R u[3]) const {
-        R g[3] = {R(p.g[0]), R(p.g[1]), R(p.g[2])};
+    void collide_node(const R* f, R* out, R& r, R u[3], R extra_gy = R(0)) const {
+        R g[3] = {R(p.g[0]), R(p.g[1]) + extra_gy, R(p.g[2])};
         moments<L, R>(f, g, r, u);
         const R tau = node_tau(f, r, u);
         if (p.collision == 0) {
@@ -531,9 +554,29 @@ struct Grid {
                 for (int q = 0; q < Q; ++q) fdst[q * n + i] = f[q];
                 continue;
             }
-            collide_node(f, o, r, u);
+            if (thermal_on()) {
+                // local Boussinesq force from this node's temperature, then the temperature collide
+                R t5[5], T = R(0);
+                for (int q = 0; q < 5; ++q) {
+                    t5[q] = tsrc[q * n + i];
+                    T += t5[q];
+                }
+                collide_node(f, o, r, u, R(p.beta_g) * (T - R(p.t_ref)));
+                const R om = R(1) / R(p.tau_t);
+                for (int q = 0; q < 5; ++q) {
+                    const R cu = R(D2Q5T::cx[q]) * u[0] + R(D2Q5T::cy[q]) * u[1];
+                    const R geq = wq<D2Q5T, R>(q) * T * (R(1) + R(3) * cu);
+                    tdst[q * n + i] = t5[q] - om * (t5[q] - geq);
+                }
+            } else {
+                collide_node(f, o, r, u);
+            }
             for (int q = 0; q < Q; ++q) fdst[q * n + i] = o[q];
         }
+        if (thermal_on())
+            for (std::size_t i = 0; i < n; ++i)
+                if (type[i] == SOLID)
+                    for (int q = 0; q < 5; ++q) tdst[q * n + i] = tsrc[q * n + i];
         // 3. pull stream f_dst -> f_src with half-way bounce-back (d2q9_streaming.ispc:33-95,
         //    d3q19_streaming.ispc:39-104)
         R mom[L::Q];
@@ -558,6 +601,29 @@ struct Grid {
                         else fsrc[q * n + i] = fdst[q * n + s];
                     }
                 }
+        // 3b. temperature: pull, anti-bounce-back through the y walls, bounce-back at solids
+        if (thermal_on()) {
+            for (int y = 0; y < ny; ++y)
+                for (int x = 0; x < nx; ++x) {
+                    const std::size_t i = at(x, y, 0);
+                    for (int q = 0; q < 5; ++q) {
+                        if (type[i] == SOLID) {
+                            tsrc[q * n + i] = tdst[q * n + i];
+                            continue;
+                        }
+                        const int o = D2Q5T::opp[q];
+                        const int sx = (x - D2Q5T::cx[q] + nx) % nx, sy = y - D2Q5T::cy[q];
+                        if (sy < 0 || sy >= ny) {
+                            const R tw = R(sy < 0 ? p.t_south : p.t_north);
+                            tsrc[q * n + i] = -tdst[o * n + i] + R(2) * wq<D2Q5T, R>(q) * tw;
+                        } else if (type[at(sx, sy, 0)] == SOLID) {
+                            tsrc[q * n + i] = tdst[o * n + i];
+                        } else {
+                            tsrc[q * n + i] = tdst[q * n + at(sx, sy, 0)];
+                        }
+                    }
+                }
+        }
         // 4. BFL curved links, reading post-collision values (d3q19_curved.ispc:7-71)
         if constexpr (L::Q == 19) {
             for (std::size_t k = 0; k < link_idx.size(); ++k) {
@@ -613,9 +679,18 @@ struct Grid {
         refresh_macro();
     }
 
+    bool thermal_on() const { return L::Q == 9 && p.thermal != 0; }
+
+    R temperature(std::size_t i) const {
+        R T = R(0);
+        for (int q = 0; q < 5; ++q) T += tsrc[q * n + i];
+        return T;
+    }
+
     void refresh_macro() {
-        R g[3] = {R(p.g[0]), R(p.g[1]), R(p.g[2])};
         for (std::size_t i = 0; i < n; ++i) {
+            R g[3] = {R(p.g[0]), R(p.g[1]), R(p.g[2])};
+            if (thermal_on()) g[1] += R(p.beta_g) * (temperature(i) - R(p.t_ref));
             R f[L::Q], r, u[3];
             for (int q = 0; q < L::Q; ++q) f[q] = fsrc[q * n + i];
             moments<L, R>(f, g, r, u);
@@ -794,6 +869,23 @@ void og_set_links(void* hp, int nl, const int* idx, const int* q, const double* 
 }
 
 // Advance nsteps; if hist is non-null and p.mem is set, write forces [nsteps][3] after each step.
+// Temperature populations [5][n] (pre-collision, the state of the next step).
+void og_set_thermal_state(void* hp, const double* t5) {
+    dispatch(static_cast<AnyGrid*>(hp), [&](auto* g) {
+        using R = typename std::remove_reference_t<decltype(g->tsrc)>::value_type;
+        for (std::size_t k = 0; k < 5 * g->n; ++k) g->tsrc[k] = g->tdst[k] = R(t5[k]);
+        g->refresh_macro();
+        return 0;
+    });
+}
+
+void og_get_temperature(void* hp, double* T) {
+    dispatch(static_cast<AnyGrid*>(hp), [&](auto* g) {
+        for (std::size_t i = 0; i < g->n; ++i) T[i] = g->temperature(i);
+        return 0;
+    });
+}
+
 void og_step(void* hp, int nsteps, double* hist) {
     dispatch(static_cast<AnyGrid*>(hp), [&](auto* g) {
         for (int s = 0; s < nsteps; ++s) {

@@ -266,3 +266,35 @@ def test_applied_smagorinsky_tau():
     f2[8] -= 1e-3
     t = oracle.lib().og_smagorinsky_tau(q, f2.ctypes.data, 1.0, 0.03, 0.0, 0.0, 0.52, 0.17)
     assert t > 0.52
+
+
+def test_thermal_conduction_state_is_exact():
+    """D2Q5 temperature between isothermal walls (anti-bounce-back at y = -1/2 and ny - 1/2): without
+    buoyancy the linear conduction profile with the fluid at rest is an exact steady state (with
+    buoyancy the density stratifies first, a transient of relative size ~beta_g)."""
+    nx, ny = 24, 12
+    o = oracle.OracleGrid(9, nx, ny, 1, 64)
+    o.configure(collision=1, tau=0.6, thermal=1, tau_t=0.6, t_ref=0.5, beta_g=0.0, t_south=1.0, t_north=0.0)
+    o.set_cell_types(np.zeros(nx * ny, np.uint8))
+    n = nx * ny
+    o.set_state(oracle.equilibrium(9, np.ones(n), np.zeros(n), np.zeros(n), None, prec=64))
+    y = (np.arange(ny) + 0.5) / ny
+    T = np.repeat(1.0 - y, nx)
+    o.set_thermal_state(np.outer(np.array([2.0, 1.0, 1.0, 1.0, 1.0]) / 6.0, T))
+    o.step(500)
+    assert np.abs(o.temperature() - T).max() < 1e-9
+    assert np.abs(o.macro()["uy"]).max() < 1e-9
+
+
+def test_thermal_energy_follows_wall_flux():
+    """With both walls at the reference temperature and a uniform start at it, nothing moves."""
+    nx, ny = 16, 8
+    o = oracle.OracleGrid(9, nx, ny, 1, 64)
+    o.configure(collision=0, tau=0.7, thermal=1, tau_t=0.8, t_ref=0.3, beta_g=1e-3, t_south=0.3, t_north=0.3)
+    o.set_cell_types(np.zeros(nx * ny, np.uint8))
+    n = nx * ny
+    o.set_state(oracle.equilibrium(9, np.ones(n), np.zeros(n), np.zeros(n), None, prec=64))
+    o.set_thermal_state(np.outer(np.array([2.0, 1.0, 1.0, 1.0, 1.0]) / 6.0, np.full(n, 0.3)))
+    o.step(200)
+    assert np.abs(o.temperature() - 0.3).max() < 1e-12
+    assert np.abs(o.macro()["ux"]).max() < 1e-12

@@ -1,7 +1,7 @@
 """ctypes binding of libwake_b200.so (C ABI in include/wake_gpu.h).
 
-The library is built in-tree (``python -m wake_b200.build`` or
-``__graft_entry__.build()``). Importing this module without it raises
+The library is built in-tree (``python wake_b200/build.py``, ``make -C
+wake_b200/csrc`` or ``__graft_entry__.build()``). Importing this module without it raises
 ImportError: there is no CPU fallback.
 """
 from __future__ import annotations
@@ -14,7 +14,7 @@ _HERE = Path(__file__).resolve().parent
 LIB_PATH = Path(os.environ.get("WAKE_B200_LIB", _HERE / "libwake_b200.so"))
 
 if not LIB_PATH.exists():
-    raise ImportError(f"wake_b200: {LIB_PATH} is missing; build it with `python -m wake_b200.build`")
+    raise ImportError(f"wake_b200: {LIB_PATH} is missing; build it with `python wake_b200/build.py`")
 
 lib = C.CDLL(str(LIB_PATH))
 
@@ -115,6 +115,9 @@ _PROTOS = {
     "wake_grid_time_bulk_launches": (I, [vp, I]),
     "wake_grid_bulk_launch_times": (I, [vp, vp, vp, vp]),
     "wake_grid_set_solid_ellipse": (I, [vp, F, F, F, F, F]),
+    "wake_grid_enable_thermal": (I, [vp, F, F, F, F, F]),
+    "wake_grid_initialize_temperature": (I, [vp, vp]),
+    "wake_grid_get_temperature": (I, [vp, vp]),
     "wake_grid_device_bytes": (LL, [vp]),
     "wake_grid_estimate_bytes": (LL, [I, I, I, I, I, I]),
     "wake_grid_release_scratch": (I, [vp]),

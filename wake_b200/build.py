@@ -1,4 +1,7 @@
-"""Build libwake_b200.so in-tree for sm_100a (``python -m wake_b200.build``)."""
+"""Build libwake_b200.so in-tree for sm_100a (``python wake_b200/build.py``).
+
+Run as a file (or load by path): importing the wake_b200 package needs the
+library this builds."""
 from __future__ import annotations
 
 import os

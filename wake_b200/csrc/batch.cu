@@ -168,6 +168,8 @@ int build_tables(wake_batch* b) {
         d.a = grid_step_args(g);
         d.buf[0] = g->A.p;
         d.buf[1] = g->B.p;
+        d.tbuf[0] = g->tbuf(0);
+        d.tbuf[1] = g->tbuf(1);
         d.cur0 = g->cur ^ b->parity;
         d.gen_first = b->gen_first[i];
         dom[i] = d;

@@ -57,10 +57,10 @@ cudaError_t launch_initial_any(int Q, int coll, int store, bool les, const float
 }
 cudaError_t launch_materialise_any(int Q, int store, const void* fin, const uint8_t* flags, const Geo& geo,
                                    const Links& links, const Physics& phys, const Out& out, const Launch& L,
-                                   int direct) {
-    if (Q == 9) return launch_materialise_q9(store, fin, flags, geo, links, phys, out, L, direct);
-    if (Q == 19) return launch_materialise_q19(store, fin, flags, geo, links, phys, out, L, direct);
-    return launch_materialise_q27(store, fin, flags, geo, links, phys, out, L, direct);
+                                   int direct, const Thermal& th) {
+    if (Q == 9) return launch_materialise_q9(store, fin, flags, geo, links, phys, out, L, direct, th);
+    if (Q == 19) return launch_materialise_q19(store, fin, flags, geo, links, phys, out, L, direct, th);
+    return launch_materialise_q27(store, fin, flags, geo, links, phys, out, L, direct, th);
 }
 cudaError_t launch_flags_any(int Q, const uint8_t* types, uint8_t* flags, const Geo& geo, const FlagCfg& cfg,
                              const Launch& L) {
@@ -220,6 +220,27 @@ __global__ void k_solid_neighbours(const uint8_t* __restrict__ types, int nx, in
     }
 }
 
+// Temperature populations at rest: g_q = w_q T (D2Q5 weights), from a per-node temperature.
+__global__ void k_t5_equilibrium(const float* __restrict__ T, float* __restrict__ t5, long long pitch, long long n) {
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const float v = T[i];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) t5[q * pitch + i] = __fmul_rn(D2Q5::w(q), v);
+    }
+}
+
+// T = sum of the temperature populations (in the order q = 0..4).
+__global__ void k_t5_sum(const float* __restrict__ t5, long long pitch, long long n, float* __restrict__ T) {
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        float t[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) t[q] = t5[q * pitch + i];
+        T[i] = sum_t5(t);
+    }
+}
+
 cudaError_t launch_link_marks(const int* link_node, int n_links, uint8_t* flags, int* node_start,
                               cudaStream_t stream) {
     if (n_links <= 0) return cudaSuccess;
@@ -287,6 +308,8 @@ int rebuild_flags(wake_grid* g) {
         cls.release();
         // general segments; pure-gather spans: whole rows, or the runs of pure-gather
         // segments of the rows that hold general segments
+        if (g->th.on)  // the coupled temperature runs on the general per-node path only
+            for (auto& c : h) c = static_cast<uint8_t>(c & ~1u);
         std::vector<unsigned> gen;
         std::vector<uint4> spans, mixed_spans;
         std::vector<uint8_t> row_fast(static_cast<std::size_t>(g->rows), 1);
@@ -457,6 +480,17 @@ int ensure_macro(wake_grid* g) {
     return WAKE_OK;
 }
 
+// Temperature view of the current state for the readers: the current post-collision
+// temperature buffer (its sum is the temperature of the reported step). Before the
+// first step the fields are reported as initialised, without the buoyancy shift.
+Thermal state_thermal(const wake_grid* g) {
+    Thermal t = g->th;
+    t.on = g->th.on && g->k > 0;
+    t.tin = t.on ? g->tbuf(g->cur) : nullptr;
+    t.tout = nullptr;
+    return t;
+}
+
 // Physics for reporting the state after the last step: the moments carry the
 // Guo shift of the body force that step used (lattice_grid_2d.cpp:257-259);
 // before any step there is none (initialize() stores the fields as given).
@@ -479,7 +513,7 @@ int materialise(wake_grid* g, bool want_f, bool want_macro) {
         if (!want_macro) return WAKE_OK;
         const Out o = scratch_out(g, false, true);
         WK_CUDA(launch_materialise_any(g->Q, STORE_F32, g->m_f.p, g->d_flags.as<uint8_t>(), g->geo(), g->links(), rp, o,
-                                       g->launch(), 1));
+                                       g->launch(), 1, state_thermal(g)));
         return WAKE_OK;
     }
     if (want_f) WK_CUDA(g->m_f.ensure(sizeof(float) * g->Q * g->pitch));
@@ -487,15 +521,25 @@ int materialise(wake_grid* g, bool want_f, bool want_macro) {
     // before the first step the other buffer holds f^0 itself (k_initial), read in place;
     // after it, f^k is re-gathered from g^{k-1}
     WK_CUDA(launch_materialise_any(g->Q, g->storage, g->buf(1 - g->cur), g->d_flags.as<uint8_t>(), g->geo(),
-                                   g->links(), rp, o, g->launch(), g->k == 0 ? 1 : 0));
+                                   g->links(), rp, o, g->launch(), g->k == 0 ? 1 : 0, state_thermal(g)));
     if (want_f) g->mf_valid = true;
     return WAKE_OK;
 }
 
 // Collide f^k (FP32 in m_f) with the current parameters: A <- Collide(f^k), B <- f^k.
 int initial_from_scratch(wake_grid* g) {
-    WK_CUDA(launch_initial_any(g->Q, g->collision, g->storage, g->les != 0, g->m_f.as<float>(), g->A.p, g->B.p,
-                               g->d_flags.as<uint8_t>(), g->geo(), g->phys, g->launch()));
+    if (g->th.on) {
+        // the temperature has no re-derivable pre-collision state, so it collides from its start only
+        if (g->k != 0 || !g->mt_valid)
+            return set_error(WAKE_ERR_INVALID, "a coupled temperature collides from its initial state only: "
+                                               "model, tau and body force are fixed once a thermal grid has stepped");
+        WK_CUDA(launch_initial_thermal_q9(g->collision, g->storage, g->les != 0, g->m_f.as<float>(), g->m_t.as<float>(),
+                                          g->A.p, g->B.p, g->tbuf(0), g->tbuf(1), g->d_flags.as<uint8_t>(), g->geo(),
+                                          g->phys, g->th, g->launch()));
+    } else {
+        WK_CUDA(launch_initial_any(g->Q, g->collision, g->storage, g->les != 0, g->m_f.as<float>(), g->A.p, g->B.p,
+                                   g->d_flags.as<uint8_t>(), g->geo(), g->phys, g->launch()));
+    }
     g->cur = 0;
     g->pending = false;
     for (int a = 0; a < 3; ++a) g->collided_g[a] = g->phys.g[a];
@@ -558,6 +602,8 @@ int do_steps(wake_grid* g, int n) {
         StepArgs a = wk::grid_step_args(g);
         a.fin = g->buf(g->cur);
         a.fout = g->buf(1 - g->cur);
+        a.th.tin = g->tbuf(g->cur);
+        a.th.tout = g->tbuf(1 - g->cur);
         if (g->use_tiles()) {
             // one persistent launch for the general rows and the staged pure-gather tiles,
             // then the momentum-exchange sum of the slots it wrote
@@ -663,6 +709,7 @@ StepArgs grid_step_args(const wake_grid* g) {
         a.mem.hist_cap = g->hist_cap;
     }
     a.phys = g->phys;
+    a.th = g->th;
     return a;
 }
 
@@ -883,6 +930,72 @@ int wake_grid_set_solid_ellipse(wake_grid* g, float cx, float cy, float a, float
                 if (u * u * inv_a2 + v * v * inv_b2 <= 1.0f) g->types[idx3(g, x, y, z)] = WAKE_CELL_SOLID;
             }
     g->geom_dirty = true;
+    return WAKE_OK;
+}
+
+int wake_grid_enable_thermal(wake_grid* g, float tau_t, float t_ref, float beta_g, float t_south, float t_north) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    if (g->Q != 9) return set_error(WAKE_ERR_INVALID, "wake_grid_enable_thermal: D2Q9 lattices only");
+    if (!(tau_t > 0.5f)) return set_error(WAKE_ERR_INVALID, "wake_grid_enable_thermal: tau_t must exceed 1/2");
+    if (g->k != 0) return set_error(WAKE_ERR_INVALID, "wake_grid_enable_thermal: only before the first step");
+    const std::size_t b = sizeof(float) * 5 * g->pitch;
+    WK_CUDA(g->TA.ensure(b));
+    WK_CUDA(g->TB.ensure(b));
+    g->th.on = 1;
+    g->th.omega_t = 1.0f / tau_t;
+    g->th.t_ref = t_ref;
+    g->th.beta_g = beta_g;
+    g->th.t_south = t_south;
+    g->th.t_north = t_north;
+    g->geom_dirty = true;  // every segment moves to the general path
+    g->pending = true;
+    g->invalidate_graph();
+    if (!g->mt_valid) {  // start from the reference temperature everywhere
+        std::vector<float> T(static_cast<std::size_t>(g->N), t_ref);
+        return wake_grid_initialize_temperature(g, T.data());
+    }
+    return WAKE_OK;
+}
+
+int wake_grid_initialize_temperature(wake_grid* g, const float* T) {
+    if (!valid_grid(g) || !T) return set_error(WAKE_ERR_INVALID, "null temperature");
+    if (!g->th.on) return set_error(WAKE_ERR_INVALID, "wake_grid_initialize_temperature: enable the temperature first");
+    if (g->k != 0 && !g->mf_valid)
+        return set_error(WAKE_ERR_INVALID, "wake_grid_initialize_temperature: initialise the flow again first");
+    WK_CUDA(g->m_t.ensure(sizeof(float) * 5 * g->pitch));
+    DevMem tmp;
+    WK_CUDA(tmp.ensure(sizeof(float) * g->N));
+    WK_CUDA(cudaMemcpyAsync(tmp.p, T, sizeof(float) * g->N, cudaMemcpyDefault, g->stream));
+    const int blocks = static_cast<int>(std::min<long long>((g->N + 255) / 256, 148ll * 16));
+    k_t5_equilibrium<<<blocks, 256, 0, g->stream>>>(tmp.as<float>(), g->m_t.as<float>(), g->pitch, g->N);
+    WK_CUDA(cudaGetLastError());
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    tmp.release();
+    g->mt_valid = true;
+    g->pending = true;
+    g->k = 0;  // a coupled run restarts from the flow state in the FP32 scratch
+    g->invalidate_graph();
+    return WAKE_OK;
+}
+
+int wake_grid_get_temperature(wake_grid* g, float* T) {
+    if (!valid_grid(g) || !T) return set_error(WAKE_ERR_INVALID, "null output");
+    if (!g->th.on) return set_error(WAKE_ERR_INVALID, "wake_grid_get_temperature: no coupled temperature");
+    DevMem tmp;
+    WK_CUDA(tmp.ensure(sizeof(float) * g->N));
+    const int blocks = static_cast<int>(std::min<long long>((g->N + 255) / 256, 148ll * 16));
+    if (g->pending || g->k == 0) {
+        // not stepped yet: the initial temperature populations
+        if (!g->mt_valid) return set_error(WAKE_ERR_INVALID, "wake_grid_get_temperature: no temperature state");
+        k_t5_sum<<<blocks, 256, 0, g->stream>>>(g->m_t.as<float>(), g->pitch, g->N, tmp.as<float>());
+    } else {
+        // BGK conserves sum g, so the current post-collision buffer sums to the step's temperature
+        k_t5_sum<<<blocks, 256, 0, g->stream>>>(g->tbuf(g->cur), g->pitch, g->N, tmp.as<float>());
+    }
+    WK_CUDA(cudaGetLastError());
+    WK_CUDA(cudaMemcpyAsync(T, tmp.p, sizeof(float) * g->N, cudaMemcpyDefault, g->stream));
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    tmp.release();
     return WAKE_OK;
 }
 
@@ -1318,13 +1431,16 @@ long long wake_grid_device_bytes(wake_grid* g) {
     const DevMem* all[] = {&g->A, &g->B, &g->d_types, &g->d_flags, &g->d_status, &g->d_nodestart, &g->d_link_node,
                            &g->d_link_q, &g->d_link_delta, &g->d_link_mom, &g->d_counters, &g->d_hist,
                            &g->d_warp_base, &g->d_contrib, &g->d_fast_rows, &g->d_gen_rows, &g->m_f, &g->m_rho,
-                           &g->m_ux, &g->m_uy, &g->m_uz, &g->m_speed, &g->m_diag};
+                           &g->m_ux, &g->m_uy, &g->m_uz, &g->m_speed, &g->m_diag, &g->TA, &g->TB, &g->m_t,
+                           &g->d_tiles, &g->d_gen4, &g->d_mixed};
     long long sum = 0;
     for (const DevMem* m : all) sum += static_cast<long long>(m->bytes);
     return sum;
 }
 
 long long wake_grid_estimate_bytes(int q, int nx, int ny, int nz, int storage, int with_fields) {
+    const bool thermal = (with_fields & 2) != 0;
+    with_fields &= 1;
     if (!(q == 9 || q == 19 || q == 27) || nx < 1 || ny < 1 || nz < 1 || storage < 0 || storage > 2)
         return set_error(WAKE_ERR_INVALID, "wake_grid_estimate_bytes: invalid lattice, size or storage");
     const long long N = static_cast<long long>(nx) * ny * nz, pitch = (N + 63) / 64 * 64;
@@ -1334,6 +1450,7 @@ long long wake_grid_estimate_bytes(int q, int nx, int ny, int nz, int storage, i
     b += 2 * N + 4 * N;                  // cell types, flags, per-node first curved link
     b += 8ll * ny * nz;                  // row lists
     if (with_fields) b += 5 * 4 * N;     // rho, ux, uy, uz, speed
+    if (thermal) b += 3 * 5 * 4 * pitch;  // coupled temperature: two state buffers and the start-up populations
     return b + (1ll << 20);              // history ring, slots and small tables
 }
 
@@ -1344,6 +1461,10 @@ int wake_grid_release_scratch(wake_grid* g) {
     WK_CUDA(cudaStreamSynchronize(g->stream));
     g->m_f.reset();
     g->mf_valid = false;
+    if (g->k > 0 || !g->pending) {  // the initial temperature populations were collided already
+        g->m_t.reset();
+        g->mt_valid = false;
+    }
     g->m_rho.reset();
     g->m_ux.reset();
     g->m_uy.reset();

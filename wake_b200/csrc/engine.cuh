@@ -121,6 +121,13 @@ struct wake_grid {
 
     DevMem m_f, m_rho, m_ux, m_uy, m_uz, m_speed, m_diag;
 
+    // coupled D2Q5 temperature (D2Q9 lattices): post-collision populations in TA / TB
+    // (same parity as A / B), FP32 start-up populations in m_t
+    wk::Thermal th{};
+    DevMem TA, TB, m_t;
+    bool mt_valid = false;
+    float* tbuf(int which) const { return static_cast<float*>(which == 0 ? TA.p : TB.p); }
+
     // CUDA graph of `graph_steps` fused steps starting from buffer parity graph_cur
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0, graph_cur = -1;
@@ -143,7 +150,7 @@ struct wake_grid {
             DevMem* all[] = {&A, &B, &d_types, &d_flags, &d_status, &d_nodestart, &d_link_node, &d_link_q,
                              &d_link_delta, &d_link_mom, &d_counters, &d_hist, &d_warp_base, &d_contrib,
                              &d_fast_rows, &d_gen_rows, &d_tiles, &d_gen4, &d_mixed, &m_f, &m_rho, &m_ux, &m_uy, &m_uz,
-                             &m_speed, &m_diag};
+                             &m_speed, &m_diag, &TA, &TB, &m_t};
             for (DevMem* m : all) m->release();
         }
         for (cudaEvent_t e : t_ev) cudaEventDestroy(e);

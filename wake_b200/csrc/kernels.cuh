@@ -35,7 +35,7 @@ struct FlagCfg {
                                   cudaStream_t stream);                                                          \
     cudaError_t launch_materialise_q##Q(int store, const void* fin, const uint8_t* flags, const Geo& geo,        \
                                         const Links& links, const Physics& phys, const Out& out,                 \
-                                        const Launch& L, int direct);                                            \
+                                        const Launch& L, int direct, const Thermal& th);                         \
     cudaError_t launch_initial_q##Q(int coll, int store, bool les, const float* f0, void* a, void* b,            \
                                     const uint8_t* flags, const Geo& geo, const Physics& phys, const Launch& L); \
     cudaError_t launch_flags_q##Q(const uint8_t* types, uint8_t* flags, const Geo& geo, const FlagCfg& cfg,      \
@@ -44,6 +44,10 @@ struct FlagCfg {
                                       cudaStream_t stream);
 
 WK_DECLARE_LAUNCHERS(9)
+// Initial collide of a D2Q9 flow with its coupled D2Q5 temperature (kernels_q9.cu).
+cudaError_t launch_initial_thermal_q9(int coll, int store, bool les, const float* f0, const float* t0, void* a, void* b,
+                                      float* ta, float* tb, const uint8_t* flags, const Geo& geo, const Physics& phys,
+                                      const Thermal& th, const Launch& L);
 WK_DECLARE_LAUNCHERS(19)
 WK_DECLARE_LAUNCHERS(27)
 

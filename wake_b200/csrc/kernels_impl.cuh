@@ -100,7 +100,7 @@ __global__ void k_seg_class(const uint8_t* __restrict__ flags, uint8_t* __restri
 // Pull-free read of f^0 (state buffer holding pre-collision populations).
 template <int Q, int S>
 __global__ void __launch_bounds__(512) k_direct(const void* fin_v, const uint8_t* flags, Geo geo, Physics phys,
-                                                Out out, int xchunks) {
+                                                Out out, int xchunks, Thermal th) {
     using L = Lat<Q>;
     using C = Codec<S>;
     const typename C::T* fin = static_cast<const typename C::T*>(fin_v);
@@ -116,8 +116,15 @@ __global__ void __launch_bounds__(512) k_direct(const void* fin_v, const uint8_t
         for (int q = 0; q < Q; ++q) out.f[q * geo.pitch + i] = f[q];
     }
     if (out.rho) {
+        float g[3] = {phys.g[0], phys.g[1], phys.g[2]};
+        if (th.on) {  // local buoyancy of the state's temperature (sum of the current temperature buffer)
+            float t5[5];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) t5[q] = th.tin[q * geo.pitch + i];
+            g[1] = buoyant_gy(th, phys.g[1], sum_t5(t5));
+        }
         float rho, u[3];
-        node_moments<Q>(f, phys.g, rho, u);
+        node_moments<Q>(f, g, rho, u);
         out.rho[i] = rho;
         out.ux[i] = u[0];
         out.uy[i] = u[1];
@@ -245,25 +252,58 @@ cudaError_t WK_CAT(launch_initial_q, WK_Q)(int coll, int store, bool les, const 
 
 cudaError_t WK_CAT(launch_materialise_q, WK_Q)(int store, const void* fin, const uint8_t* flags, const Geo& geo,
                                               const Links& links, const Physics& phys, const Out& out,
-                                              const Launch& L, int direct) {
+                                              const Launch& L, int direct, const Thermal& th) {
     const int blocks = L.rows * L.xchunks;
     if (direct) {
         switch (store) {
-            case 0: k_direct<kQ, 0><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, phys, out, L.xchunks); break;
-            case 1: k_direct<kQ, 1><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, phys, out, L.xchunks); break;
-            case 2: k_direct<kQ, 2><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, phys, out, L.xchunks); break;
+            case 0: k_direct<kQ, 0><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, phys, out, L.xchunks, th); break;
+            case 1: k_direct<kQ, 1><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, phys, out, L.xchunks, th); break;
+            case 2: k_direct<kQ, 2><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, phys, out, L.xchunks, th); break;
             default: return cudaErrorInvalidValue;
         }
     } else {
         switch (store) {
-            case 0: k_materialise<kQ, 0><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, links, phys, out, L.xchunks); break;
-            case 1: k_materialise<kQ, 1><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, links, phys, out, L.xchunks); break;
-            case 2: k_materialise<kQ, 2><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, links, phys, out, L.xchunks); break;
+            case 0: k_materialise<kQ, 0><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, links, phys, out, L.xchunks, th); break;
+            case 1: k_materialise<kQ, 1><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, links, phys, out, L.xchunks, th); break;
+            case 2: k_materialise<kQ, 2><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, links, phys, out, L.xchunks, th); break;
             default: return cudaErrorInvalidValue;
         }
     }
     return cudaGetLastError();
 }
+
+#if WK_Q == 9
+cudaError_t launch_initial_thermal_q9(int coll, int store, bool les, const float* f0, const float* t0, void* a, void* b,
+                                      float* ta, float* tb, const uint8_t* flags, const Geo& geo, const Physics& phys,
+                                      const Thermal& th, const Launch& L) {
+    if (!valid(coll, store)) return cudaErrorInvalidValue;
+    const int blocks = L.rows * L.xchunks;
+#define WK_TI(C, S, LES) \
+    k_initial_thermal<C, S, LES><<<blocks, L.tpb, 0, L.stream>>>(f0, t0, a, b, ta, tb, flags, geo, phys, th, L.xchunks)
+    switch (coll * 6 + store * 2 + (les ? 1 : 0)) {
+        case 0: WK_TI(0, 0, false); break;
+        case 1: WK_TI(0, 0, true); break;
+        case 2: WK_TI(0, 1, false); break;
+        case 3: WK_TI(0, 1, true); break;
+        case 4: WK_TI(0, 2, false); break;
+        case 5: WK_TI(0, 2, true); break;
+        case 6: WK_TI(1, 0, false); break;
+        case 7: WK_TI(1, 0, true); break;
+        case 8: WK_TI(1, 1, false); break;
+        case 9: WK_TI(1, 1, true); break;
+        case 10: WK_TI(1, 2, false); break;
+        case 11: WK_TI(1, 2, true); break;
+        case 12: WK_TI(2, 0, false); break;
+        case 13: WK_TI(2, 0, true); break;
+        case 14: WK_TI(2, 1, false); break;
+        case 15: WK_TI(2, 1, true); break;
+        case 16: WK_TI(2, 2, false); break;
+        default: WK_TI(2, 2, true); break;
+    }
+#undef WK_TI
+    return cudaGetLastError();
+}
+#endif
 
 cudaError_t WK_CAT(launch_flags_q, WK_Q)(const uint8_t* types, uint8_t* flags, const Geo& geo, const FlagCfg& cfg,
                                         const Launch& L) {

@@ -97,6 +97,8 @@ __device__ __forceinline__ StepArgs tile_member(const StepArgs& a, const TileArg
         const int c = d->cur0 ^ t.parity;
         r.fin = d->buf[c];
         r.fout = d->buf[c ^ 1];
+        r.th.tin = d->tbuf[c];
+        r.th.tout = d->tbuf[c ^ 1];
         return r;
     } else {
         (void)t;

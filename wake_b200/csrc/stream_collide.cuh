@@ -209,6 +209,66 @@ __device__ __forceinline__ void mem_node(const float* f, unsigned bb, int x, int
     }
 }
 
+// D2Q5 temperature coupled to a D2Q9 flow (no reference counterpart; the
+// reference's thermal solver uses a D2Q9 temperature and one domain-averaged
+// force, src/thermal/thermal_solver.cpp:83-123, src/scenarios/thermal_convection.cpp:70).
+// Per node: T = sum g, the flow collides with the body force g + (0, beta_g (T - T_ref)),
+// the temperature relaxes to w_q T (1 + 3 c_q.u) with omega_t (first-order equilibrium
+// as thermal_kernels.ispc:32). Streaming: anti-bounce-back g_q = -g*_opp + 2 w_q T_wall
+// through the y walls (Dirichlet), bounce-back at solid nodes (adiabatic).
+struct Thermal {
+    int on;
+    float omega_t, t_ref, beta_g, t_south, t_north;
+    const float* tin;  // post-collision temperature populations of the last step [5][pitch]
+    float* tout;
+};
+
+struct D2Q5 {  // rest, +x, +y, -x, -y; c_s^2 = 1/3
+    __host__ __device__ static constexpr int cx(int q) { return q == 1 ? 1 : (q == 3 ? -1 : 0); }
+    __host__ __device__ static constexpr int cy(int q) { return q == 2 ? 1 : (q == 4 ? -1 : 0); }
+    __host__ __device__ static constexpr int opp(int q) { return q == 0 ? 0 : (q + 1) % 4 + 1; }
+    __host__ __device__ static constexpr float w(int q) { return q == 0 ? 1.0f / 3.0f : 1.0f / 6.0f; }
+};
+
+// Pull the temperature populations of node (x, y) (2D, i its index).
+__device__ __forceinline__ void gather_t5(const Thermal& th, const uint8_t* __restrict__ flags, const Geo& G,
+                                          long long P, int x, int y, long long i, float t[5]) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        const int o = D2Q5::opp(q);
+        const int sx = D2Q5::cx(q) ? wrap<9>(x - D2Q5::cx(q), G.nx) : x, sy = y - D2Q5::cy(q);
+        if (sy < 0 || sy >= G.ny) {
+            const float tw = sy < 0 ? th.t_south : th.t_north;
+            t[q] = __fadd_rn(-th.tin[o * P + i], __fmul_rn(2.0f * D2Q5::w(q), tw));
+        } else {
+            const long long s = static_cast<long long>(sy) * G.nx + sx;
+            t[q] = ((flags[s] & FL_TYPE) == CT_SOLID) ? th.tin[o * P + i] : th.tin[q * P + s];
+        }
+    }
+}
+
+__device__ __forceinline__ float sum_t5(const float t[5]) {
+    float T = t[0];
+#pragma unroll
+    for (int q = 1; q < 5; ++q) T = __fadd_rn(T, t[q]);
+    return T;
+}
+
+// Body force of a node with temperature T: g + (0, beta_g (T - T_ref), 0), explicit roundings.
+__device__ __forceinline__ float buoyant_gy(const Thermal& th, float gy, float T) {
+    return __fadd_rn(gy, __fmul_rn(th.beta_g, __fsub_rn(T, th.t_ref)));
+}
+
+// BGK relaxation of the temperature populations toward w_q T (1 + 3 c_q.u).
+__device__ __forceinline__ void collide_t5(float t[5], float T, const float u[3], float om) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        const float cu = __fadd_rn(__fmul_rn(float(D2Q5::cx(q)), u[0]), __fmul_rn(float(D2Q5::cy(q)), u[1]));
+        const float geq = __fmul_rn(__fmul_rn(D2Q5::w(q), T), __fadd_rn(1.0f, __fmul_rn(3.0f, cu)));
+        t[q] = __fsub_rn(t[q], __fmul_rn(om, __fsub_rn(t[q], geq)));
+    }
+}
+
 struct StepArgs {
     const void* fin;
     void* fout;
@@ -222,6 +282,7 @@ struct StepArgs {
     int nrows;
     const uint4* spans;    // pure-gather spans (member, row, x0, x1); one block per span
     int nspans;
+    Thermal th;            // D2Q9 lattices only; th.on = 0 otherwise
 };
 
 // Work unit of the step kernels: a segment of up to SEG consecutive nodes of one
@@ -292,8 +353,17 @@ __device__ __forceinline__ void step_chunk(const StepArgs& a, unsigned e, int en
         float f[Q];
         unsigned bb;
         gather<Q, S>(static_cast<const T*>(a.fin), a.geo, a.flags, a.links, x, y, z, i, fl, f, bb);
+        Physics ph = a.phys;  // a coupled temperature adds the node's buoyancy to the body force
+        float t5[5], Tn = 0.f;
+        if constexpr (Q == 9) {
+            if (a.th.on) {
+                gather_t5(a.th, a.flags, a.geo, a.geo.pitch, x, y, i, t5);
+                Tn = sum_t5(t5);
+                ph.g[1] = buoyant_gy(a.th, a.phys.g[1], Tn);
+            }
+        }
         float rho, u[3];
-        node_moments<Q>(f, a.phys.g, rho, u);
+        node_moments<Q>(f, ph.g, rho, u);
         if (slot >= 0) {
             double acc[3] = {0.0, 0.0, 0.0};
             mem_node<Q>(f, bb, x, y, z, a.geo, a.mem, acc);
@@ -303,10 +373,17 @@ __device__ __forceinline__ void step_chunk(const StepArgs& a, unsigned e, int en
             c[2] = acc[2];
         }
         if (!(rho > 0.0f) || !(fabsf(u[0]) < 1e30f)) atomicOr(a.status, ERR_NONFINITE);
-        collide<Q, COLL, LES>(f, rho, u, a.phys);
+        collide<Q, COLL, LES>(f, rho, u, ph);
         T* out = static_cast<T*>(a.fout);
 #pragma unroll
         for (int q = 0; q < Q; ++q) C::store_stream(out + q * a.geo.pitch + i, f[q], L::w(q));
+        if constexpr (Q == 9) {
+            if (a.th.on) {
+                collide_t5(t5, Tn, u, a.th.omega_t);
+#pragma unroll
+                for (int q = 0; q < 5; ++q) __stcs(a.th.tout + q * a.geo.pitch + i, t5[q]);
+            }
+        }
     }
 }
 
@@ -499,8 +576,9 @@ __global__ void __launch_bounds__(256, COLL == COLL_TRT ? 2 : 4) k_step_fast(con
 // Each member's step arguments live in device memory; its buffers swap with the
 // batch's step parity, so the table stays valid while the members step together.
 struct BatchDom {
-    StepArgs a;        // fin / fout unused: taken from buf[] by parity
+    StepArgs a;        // fin / fout (th.tin / th.tout) unused: taken from buf[] (tbuf[]) by parity
     void* buf[2];      // the member's two state buffers
+    float* tbuf[2];    // its two temperature buffers (thermal members)
     int cur0;          // index of the buffer holding the state at batch parity 0
     int gen_first;     // first entry of this member in the general-row list
 };
@@ -520,6 +598,8 @@ __device__ __forceinline__ StepArgs batch_member(const BatchArgs& b, unsigned m)
     const int c = d->cur0 ^ b.parity;
     a.fin = d->buf[c];
     a.fout = d->buf[c ^ 1];
+    a.th.tin = d->tbuf[c];
+    a.th.tout = d->tbuf[c ^ 1];
     return a;
 }
 
@@ -569,7 +649,7 @@ __device__ __forceinline__ void mem_reduce_block(const double* __restrict__ cont
 // lattice_grid_2d.cpp:257-262). Solid nodes report their frozen populations.
 template <int Q, int S>
 __global__ void __launch_bounds__(512) k_materialise(const void* fin_v, const uint8_t* flags, Geo geo, Links links,
-                                                     Physics phys, Out out, int xchunks) {
+                                                     Physics phys, Out out, int xchunks, Thermal th) {
     using L = Lat<Q>;
     using C = Codec<S>;
     using T = typename C::T;
@@ -593,14 +673,62 @@ __global__ void __launch_bounds__(512) k_materialise(const void* fin_v, const ui
         for (int q = 0; q < Q; ++q) out.f[q * geo.pitch + i] = f[q];
     }
     if (out.rho) {
+        float g[3] = {phys.g[0], phys.g[1], phys.g[2]};
+        if (th.on) {  // the step's local buoyancy: T^k is the sum of the current post-collision temperature
+            float t5[5];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) t5[q] = th.tin[q * geo.pitch + i];
+            g[1] = buoyant_gy(th, phys.g[1], sum_t5(t5));
+        }
         float rho, u[3];
-        node_moments<Q>(f, phys.g, rho, u);
+        node_moments<Q>(f, g, rho, u);
         out.rho[i] = rho;
         out.ux[i] = u[0];
         out.uy[i] = u[1];
         if (out.uz) out.uz[i] = u[2];
         out.speed[i] = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
     }
+}
+
+// Initial collide of a coupled flow + temperature state (f^0 and T populations
+// g^0 in FP32 scratch): A <- Collide(f^0) with the local buoyancy, TA <- Collide_T(g^0);
+// B <- f^0, TB <- g^0. Solid nodes copy through.
+template <int COLL, int S, bool LES>
+__global__ void __launch_bounds__(512) k_initial_thermal(const float* f0, const float* t0, void* a_v, void* b_v,
+                                                         float* ta, float* tb, const uint8_t* flags, Geo geo,
+                                                         Physics phys, Thermal th, int xchunks) {
+    using L = Lat<9>;
+    using C = Codec<S>;
+    using T = typename C::T;
+    const int row = blockIdx.x / xchunks;
+    const int x = (blockIdx.x - row * xchunks) * blockDim.x + threadIdx.x;
+    if (x >= geo.nx) return;
+    const long long i = static_cast<long long>(row) * geo.nx + x;
+    const long long P = geo.pitch;
+    float f[9], t5[5];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[q] = f0[q * P + i];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) t5[q] = t0[q * P + i];
+    T* A = static_cast<T*>(a_v);
+    T* Bf = static_cast<T*>(b_v);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) C::store(Bf + q * P + i, f[q], L::w(q));
+#pragma unroll
+    for (int q = 0; q < 5; ++q) tb[q * P + i] = t5[q];
+    if ((flags[i] & FL_TYPE) != CT_SOLID) {
+        const float Tn = sum_t5(t5);
+        Physics ph = phys;
+        ph.g[1] = buoyant_gy(th, phys.g[1], Tn);
+        float rho, u[3];
+        node_moments<9>(f, ph.g, rho, u);
+        collide<9, COLL, LES>(f, rho, u, ph);
+        collide_t5(t5, Tn, u, th.omega_t);
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) C::store(A + q * P + i, f[q], L::w(q));
+#pragma unroll
+    for (int q = 0; q < 5; ++q) ta[q * P + i] = t5[q];
 }
 
 // Initial collide from FP32 populations f^0: buffer A <- g^0 = Collide(f^0)

@@ -239,6 +239,36 @@ class LatticeGrid2D(_Grid):
     def set_moving_wall_north(self, u_wall_x) -> None:
         check(lib.wake_grid_set_moving_wall(self._h, u_wall_x, 0.0, 0.0))
 
+    # -- coupled temperature (D2Q5 with local Boussinesq force; see wake_grid_enable_thermal)
+    def enable_thermal(self, tau_thermal: float, t_ref: float = 0.5, beta_g: float = 0.0,
+                       t_hot_south: float = 1.0, t_cold_north: float = 0.0) -> None:
+        """Couple a temperature field to the flow: buoyancy beta_g (T - t_ref) along +y per node,
+        isothermal walls y = -1/2 (t_hot_south) and y = ny - 1/2 (t_cold_north). Before the first step."""
+        check(lib.wake_grid_enable_thermal(self._h, tau_thermal, t_ref, beta_g, t_hot_south, t_cold_north))
+        self._thermal = (float(t_hot_south), float(t_cold_north))
+
+    def initialize_temperature(self, T) -> None:
+        arr = np.ascontiguousarray(T, dtype=np.float32).ravel()
+        check(lib.wake_grid_initialize_temperature(self._h, addr(arr)))
+
+    def temperature_data(self) -> np.ndarray:
+        out = np.empty(self.total_nodes(), np.float32)
+        check(lib.wake_grid_get_temperature(self._h, addr(out)))
+        return out
+
+    def compute_nusselt_number(self) -> float:
+        """Hot-wall Nusselt number: mean temperature drop between the first two rows over the
+        conduction drop (the form of ThermalSolver2D::compute_nusselt_number,
+        src/thermal/thermal_solver.cpp:131-146). The walls here sit half a cell outside the
+        first and last rows, so conduction drops (t_hot - t_cold) / ny per row, where the
+        reference, whose walls are the first and last rows, divides by ny - 1."""
+        t_hot, t_cold = getattr(self, "_thermal", (1.0, 0.0))
+        if abs(t_hot - t_cold) < 1e-6 or self.ny <= 1:
+            return 1.0
+        T = self.temperature_data().reshape(self.ny, self.nx).astype(np.float64)
+        mean_grad = float(np.mean(T[0] - T[1]))
+        return mean_grad / ((t_hot - t_cold) / self.ny)
+
 
 class LatticeGrid3D(_Grid):
     """GPU counterpart of wake::LatticeGrid3D (src/grid/lattice_grid_3d.cpp:46-410).

@@ -237,6 +237,32 @@ def ellipse_sweep(n_domains: int = 512, nx_range=(64, 512), seed: int = BASE_SEE
     return cases
 
 
+def rayleigh_benard(nx: int = 128, ny: int = 64, rayleigh: float = 1e4, prandtl: float = 0.71,
+                    t_hot: float = 1.0, t_cold: float = 0.0, u_free_fall: float = 0.05, noise: float = 1e-3,
+                    collision: int = 1, les: bool = True, cs_smag: float = 0.17, seed: int = BASE_SEED) -> Case:
+    """Rayleigh-Benard cell: fluid at rest between a hot wall at y = -1/2 and a cold wall at
+    y = ny - 1/2, x periodic, D2Q5 temperature with local Boussinesq buoyancy.
+
+    Parameters as ThermalConvectionScenario (src/scenarios/thermal_convection.cpp:40-48):
+    nu * alpha = g beta dT h^3 / Ra, nu = sqrt(nu alpha Pr), alpha = nu / Pr, tau = 3 nu + 1/2,
+    with h = ny and g beta = u_ff^2 / (dT h) (free-fall velocity u_ff). The start is the
+    conduction profile plus noise * (2 r - 1) from SplitMix64(seed) to trigger convection.
+    """
+    dT = t_hot - t_cold
+    gbeta = u_free_fall ** 2 / (dT * ny)
+    nu_alpha = gbeta * dT * ny ** 3 / rayleigh
+    nu = math.sqrt(nu_alpha * prandtl)
+    alpha = nu / prandtl
+    y = (np.arange(ny, dtype=np.float64) + 0.5) / ny
+    T = np.repeat(t_hot - dT * y, nx).astype(np.float32)
+    T = (T + np.float32(noise) * (np.float32(2.0) * uniform24(seed, nx * ny) - np.float32(1.0))).astype(np.float32)
+    t_ref = 0.5 * (t_hot + t_cold)
+    return Case(q=9, nx=nx, ny=ny, nz=1, types=np.zeros(nx * ny, np.uint8), init=("uniform", 1.0, (0.0, 0.0, 0.0)),
+                tau=0.5 + 3.0 * nu, collision=collision, les=les, cs_smag=cs_smag, u_ref=u_free_fall,
+                extra={"thermal": {"tau_t": 0.5 + 3.0 * alpha, "t_ref": t_ref, "beta_g": gbeta, "t_south": t_hot,
+                                   "t_north": t_cold}, "T0": T, "ra": rayleigh, "pr": prandtl})
+
+
 def sphere_channel(nx=256, ny=128, nz=128, radius=12.0, center=(64.0, 64.0, 64.0), u_in=0.05, tau=0.52,
                    collision=1, les=True, cs_smag=0.17, reference_variant=False) -> Case:
     """3D sphere in a channel.
@@ -328,4 +354,9 @@ def build_grid(case: Case, storage: str = "f32", les_applies: bool = True):
         g.build_curved_sphere_links(*case.sphere)
     if case.mem is not None:
         g.enable_forces(*case.mem)
+    th = case.extra.get("thermal")
+    if th is not None:
+        g.enable_thermal(th["tau_t"], th["t_ref"], th["beta_g"], th["t_south"], th["t_north"])
+        if case.extra.get("T0") is not None:
+            g.initialize_temperature(case.extra["T0"])
     return g
