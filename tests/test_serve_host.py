@@ -24,12 +24,14 @@ def test_mixed_jobs_distribution():
     assert abs(np.percentile(steps, 5) / 500.0 - 1.0) < 0.15
     frac3d = np.mean([j.kind == "d3q19" for j in jobs])
     assert abs(frac3d - 0.5) < 0.05
+    n2 = [j for j in jobs if j.kind != "d3q19"]
+    assert abs(np.mean([j.kind == "thermal" for j in n2]) - 0.1) < 0.03
     n3 = np.array([j.dims[1] for j in jobs if j.kind == "d3q19"])
     assert n3.min() >= 48 and n3.max() <= 160 and all(j.dims[1] == j.dims[2] == j.dims[3] for j in jobs
                                                        if j.kind == "d3q19")
-    nx2 = np.array([j.dims[1] for j in jobs if j.kind == "d2q9"])
+    nx2 = np.array([j.dims[1] for j in jobs if j.kind != "d3q19"])
     assert nx2.min() >= 64 and nx2.max() <= 512
-    assert all(j.dims[2] == j.dims[1] // 2 for j in jobs if j.kind == "d2q9")
+    assert all(j.dims[2] == j.dims[1] // 2 for j in jobs if j.kind != "d3q19")
     gaps = np.diff([0.0] + [j.arrival for j in jobs])
     assert abs(gaps.mean() * 100.0 - 1.0) < 0.1  # Poisson process at 100 jobs/s
 
@@ -53,3 +55,13 @@ def test_memory_estimate_covers_state_buffers():
             assert S.lib.wake_grid_estimate_bytes(q, *dims, storage, 1) == est + 20 * n
     assert S.lib.wake_grid_estimate_bytes(10, 8, 8, 8, 0, 0) < 0
     S.lib.wake_gpu_clear_error()
+
+
+def test_thermal_jobs_build_rayleigh_benard_cells():
+    jobs = [j for j in S.mixed_jobs(400, 50.0) if j.kind == "thermal"]
+    assert jobs
+    for j in jobs[:5]:
+        c = j.make()
+        assert (c.nx, c.ny) == (j.dims[1], j.dims[2]) and "thermal" in c.extra
+        assert 1e4 <= c.extra["ra"] <= 1e6 and c.tau - 0.5 >= 0.0079 and c.extra["thermal"]["tau_t"] > 0.5
+        assert S.job_bytes(j, "f32") > S.lib.wake_grid_estimate_bytes(9, c.nx, c.ny, 1, 0, 0)

@@ -37,7 +37,7 @@ class Job:
     long arrival list costs no host memory until its jobs are admitted."""
 
     id: int
-    kind: str            # "d2q9" | "d3q19"
+    kind: str            # "d2q9" | "thermal" | "d3q19"
     dims: tuple          # (q, nx, ny, nz)
     make: object         # () -> workloads.Case
     steps: int
@@ -66,6 +66,7 @@ class JobResult:
     diagnostics: tuple           # (mass, kinetic energy, max speed) in FP64 over fluid nodes
     error: str | None = None
     nodes: int = 0
+    nusselt: float | None = None  # Rayleigh-Benard jobs: hot-wall Nusselt number at the end
 
     @property
     def latency(self) -> float:
@@ -108,20 +109,33 @@ def sphere_job_case(n: int, storage_les: bool = True) -> W.Case:
     return W.sphere_channel(nx=n, ny=n, nz=n, radius=r, center=(n / 4.0, n / 2.0, n / 2.0), les=storage_les)
 
 
+def thermal_job_case(nx: int, rayleigh: float, seed: int) -> W.Case:
+    """Rayleigh-Benard cell nx x nx/2, Pr = 0.71 (D2Q9 flow + D2Q5 temperature), TRT + Smagorinsky."""
+    ny = nx // 2
+    return W.rayleigh_benard(nx, ny, rayleigh, 0.71, u_free_fall=W.rb_free_fall_velocity(ny, rayleigh), seed=seed)
+
+
 def mixed_jobs(n_jobs: int, rate: float, seed: int = W.BASE_SEED, d3q19_frac: float = 0.5,
                n_range=(48, 160), nx_range=(64, 512), median_steps: float = 2000.0, p5_steps: float = 500.0,
-               steps_range=(200, 20000)) -> list:
-    """Poisson arrivals at `rate` jobs/s of D2Q9 channel jobs (the ellipse sweep's domains) and D3Q19
-    sphere jobs (n^3, n ~ U[n_range]); steps lognormal (median 2000, 5th percentile 500, clipped).
-    Job j draws its inter-arrival time, kind, size and steps from SplitMix64(seed + 1_000_000 + j)."""
+               steps_range=(200, 20000), thermal_frac: float = 0.1, ra_range=(1e4, 1e6)) -> list:
+    """Poisson arrivals at `rate` jobs/s of D2Q9 jobs and D3Q19 sphere jobs (n^3, n ~ U[n_range]);
+    steps lognormal (median 2000, 5th percentile 500, clipped). A D2Q9 job is a Rayleigh-Benard cell
+    (NX ~ U[nx_range], NY = NX/2, Ra log-uniform in ra_range, Pr = 0.71) with probability
+    thermal_frac, else a channel of the ellipse sweep. Job j draws its inter-arrival time, kind, size,
+    steps and Ra from SplitMix64(seed + 1_000_000 + j)."""
     jobs, t = [], 0.0
     for j in range(n_jobs):
-        u = W.uniform24(seed + 1_000_000 + j, 6).astype(np.float64)
+        u = W.uniform24(seed + 1_000_000 + j, 7).astype(np.float64)
         t += -math.log(max(1.0 - u[0], 1e-12)) / rate
         steps = lognormal_steps(u[1], u[2], median_steps, p5_steps, *steps_range)
         if u[3] < d3q19_frac:
             n = int(n_range[0] + math.floor(u[4] * (n_range[1] - n_range[0] + 1)))
             jobs.append(Job(j, "d3q19", (19, n, n, n), (lambda n=n: sphere_job_case(n)), steps, t, (1, True, 0.17)))
+        elif u[5] < thermal_frac:
+            nx = int(nx_range[0] + math.floor(u[4] * (nx_range[1] - nx_range[0] + 1)))
+            ra = ra_range[0] * (ra_range[1] / ra_range[0]) ** u[6]
+            make = (lambda nx=nx, ra=ra, j=j: thermal_job_case(nx, ra, seed + j))
+            jobs.append(Job(j, "thermal", (9, nx, nx // 2, 1), make, steps, t, (1, True, 0.17)))
         else:
             nx = W.ellipse_sweep_dims(j, nx_range=nx_range, seed=seed)
             make = (lambda j=j: W.ellipse_sweep(1, nx_range=nx_range, seed=seed, first=j)[0])
@@ -131,7 +145,8 @@ def mixed_jobs(n_jobs: int, rate: float, seed: int = W.BASE_SEED, d3q19_frac: fl
 
 def job_bytes(job: Job, storage: str) -> int:
     q, nx, ny, nz = job.dims
-    return int(lib.wake_grid_estimate_bytes(q, nx, ny, nz, STORAGE[storage], 0))
+    flags = 2 if job.kind == "thermal" else 0  # bit 1: the coupled temperature's buffers
+    return int(lib.wake_grid_estimate_bytes(q, nx, ny, nz, STORAGE[storage], flags))
 
 
 def _class_key(job: Job):
@@ -147,14 +162,17 @@ def _start(job: Job, storage: str):
 def _finish(job: Job, g, arrival, admitted, now, error=None) -> JobResult:
     forces = np.zeros((0, 3))
     diag = (math.nan, math.nan, math.nan)
+    nusselt = None
     if error is None:
         try:
             g.synchronize()
             forces = g.force_history()
             diag = g._diag()
+            if job.kind == "thermal":
+                nusselt = g.compute_nusselt_number()
         except Exception as e:  # a job that went non-finite reports its error, the others carry on
             error = str(e)
-    return JobResult(job.id, job.kind, job.steps, arrival, admitted, now, forces, diag, error, job.nodes)
+    return JobResult(job.id, job.kind, job.steps, arrival, admitted, now, forces, diag, error, job.nodes, nusselt)
 
 
 # ------------------------------------------------------------------ server

@@ -237,6 +237,12 @@ def ellipse_sweep(n_domains: int = 512, nx_range=(64, 512), seed: int = BASE_SEE
     return cases
 
 
+def rb_free_fall_velocity(ny: int, rayleigh: float, prandtl: float = 0.71) -> float:
+    """Free-fall velocity of a Rayleigh-Benard cell: 0.05, raised (at most to 0.1) until the
+    flow's tau - 1/2 = 3 u_ff ny sqrt(Pr / Ra) reaches 0.01, so coarse high-Ra cells stay stable."""
+    return min(0.1, max(0.05, 0.01 / (3.0 * ny * math.sqrt(prandtl / rayleigh))))
+
+
 def rayleigh_benard(nx: int = 128, ny: int = 64, rayleigh: float = 1e4, prandtl: float = 0.71,
                     t_hot: float = 1.0, t_cold: float = 0.0, u_free_fall: float = 0.05, noise: float = 1e-3,
                     collision: int = 1, les: bool = True, cs_smag: float = 0.17, seed: int = BASE_SEED) -> Case:
