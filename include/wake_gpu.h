@@ -354,6 +354,34 @@ int wake_batch_info(wake_batch* b, long long* nodes, int* bulk_rows, int* genera
  * fastest; members advance 3 * steps. Results do not depend on the choice. */
 int wake_batch_autotune(wake_batch* b, int steps, int* best_threads);
 
+/* ------------------------------------------------------------------ telemetry files
+ * The reference's telemetry formats (wake::TelemetryExporter,
+ * src/export/csv_telemetry.cpp:21-125): aerodynamic CSV
+ * "step,time,fx,fy,fz,cd,cl,cm", performance CSV
+ * "step,step_time_ms,mlups,max_speed,total_mass,kinetic_energy" and the summary
+ * JSON, identical bytes for identical records. Coefficients follow
+ * compute_aerodynamic_coefficients (include/wake/forces/momentum_exchange.hpp:20-37)
+ * in float. record_history turns a grid's FP64 force history (n rows of
+ * Fx, Fy, Tz in 2D / Fx, Fy, Fz in 3D, row i = step first_step + i) into records
+ * of the steps divisible by `every` (the scenarios record every 10th step,
+ * src/scenarios/karman_vortex.cpp:126). Host code only; no device work. */
+typedef struct wake_telemetry wake_telemetry;
+wake_telemetry* wake_telemetry_create(void);
+void wake_telemetry_destroy(wake_telemetry* t);
+void wake_telemetry_clear(wake_telemetry* t);
+int wake_telemetry_record_aero(wake_telemetry* t, unsigned long long step, float time, float fx, float fy, float fz,
+                               float torque_z, float rho_inf, float u_inf, float area, float chord);
+int wake_telemetry_record_history(wake_telemetry* t, const double* hist, int n, long long first_step, int every,
+                                  int is3d, float rho_inf, float u_inf, float area, float chord);
+int wake_telemetry_record_performance(wake_telemetry* t, unsigned long long step, double step_time_ms, double mlups,
+                                      float max_speed, float total_mass, float kinetic_energy);
+int wake_telemetry_count(wake_telemetry* t, int which); /* 0: aerodynamic records, 1: performance records */
+int wake_telemetry_get_coefficients(wake_telemetry* t, int i, float* cd_cl_cm);
+int wake_telemetry_write_aero_csv(wake_telemetry* t, const char* path);
+int wake_telemetry_write_performance_csv(wake_telemetry* t, const char* path);
+int wake_telemetry_write_summary_json(wake_telemetry* t, const char* path, const char* simulation_name,
+                                      float strouhal_number, float shedding_frequency);
+
 /* FP64 Strouhal frequency of a lift history (strouhal_analyzer.cpp:39-84:
  * mean removed, Hann window over the first min(n, 4096) samples, radix-2 FFT,
  * peak bin >= 1). Returns the frequency; St = f D / U. */

@@ -13,9 +13,11 @@ C++ at build time:
 
 Nothing else is changed: every arithmetic expression is the reference's own.
 The translated files are written to ``oracle/_ref/gen`` and compiled with g++
-(-O3 -march=x86-64-v3 -ffast-math, mirroring ISPC's avx2 fast-math build)
+(-O3 -march=x86-64-v3 -ffast-math, mirroring ISPC's avx2 fast-math build; the host
+sources with the reference's own C++ flags, -O3 -pthread)
 together with the reference's host C++ compiled from where it lies
-(src/grid/lattice_grid_2d.cpp, src/grid/lattice_grid_3d.cpp, src/core/memory.cpp)
+(src/grid/lattice_grid_2d.cpp, src/grid/lattice_grid_3d.cpp, src/core/memory.cpp,
+src/forces/strouhal_analyzer.cpp, src/export/csv_telemetry.cpp)
 and the thin extern "C" shim ``oracle/ref_shim.cpp``. The output is
 ``oracle/_ref/libwake_ref.so``. Nothing is copied into the repository: the
 output directory is git-ignored.
@@ -76,11 +78,25 @@ def build(verbose: bool = False) -> Path:
     host = [ref / "src" / "grid" / "lattice_grid_2d.cpp",
             ref / "src" / "grid" / "lattice_grid_3d.cpp",
             ref / "src" / "core" / "memory.cpp",
-            ref / "src" / "forces" / "strouhal_analyzer.cpp"]
+            ref / "src" / "forces" / "strouhal_analyzer.cpp",
+            ref / "src" / "export" / "csv_telemetry.cpp"]
     so = OUT / "libwake_ref.so"
-    cmd = ["g++", "-std=c++20", "-O3", "-march=x86-64-v3", "-ffast-math", "-fPIC", "-shared",
-           f"-I{GEN / 'include'}", f"-I{ref / 'include'}",
-           *cpp_files, *map(str, host), str(HERE / "ref_shim.cpp"), "-o", str(so)]
+    # the translated kernels with ISPC's fast-math avx2 settings (CMakeLists.txt:24), the
+    # host sources with the reference's C++ flags (CMakeLists.txt:25)
+    objs = OUT / "obj"
+    objs.mkdir(parents=True, exist_ok=True)
+    inc = [f"-I{GEN / 'include'}", f"-I{ref / 'include'}"]
+    jobs = []
+    for src in cpp_files:
+        jobs.append(["g++", "-std=c++20", "-O3", "-march=x86-64-v3", "-ffast-math", "-fPIC", *inc, "-c", src, "-o",
+                     str(objs / (Path(src).stem + ".kern.o"))])
+    for src in [*map(str, host), str(HERE / "ref_shim.cpp")]:
+        jobs.append(["g++", "-std=c++20", "-O3", "-pthread", "-fPIC", *inc, "-c", src, "-o",
+                     str(objs / (Path(src).stem + ".host.o"))])
+    procs = [subprocess.Popen(c) for c in jobs]
+    if any(p.wait() != 0 for p in procs):
+        raise RuntimeError("reference build failed")
+    cmd = ["g++", "-shared", "-pthread", *[c[-1] for c in jobs], "-o", str(so)]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

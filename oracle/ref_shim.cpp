@@ -16,6 +16,7 @@
 #include "wake/grid/lattice_grid_3d.hpp"
 #undef private
 #include "wake/forces/strouhal_analyzer.hpp"
+#include "wake/export/csv_telemetry.hpp"
 
 namespace ispc {
 extern "C" {
@@ -177,6 +178,32 @@ float ref3d_total_mass(void* h) { return static_cast<LatticeGrid3D*>(h)->compute
 float ref3d_total_ke(void* h) { return static_cast<LatticeGrid3D*>(h)->compute_total_kinetic_energy(); }
 
 // ---------------------------------------------------------------- Strouhal FFT
+// ---------------------------------------------------------------- telemetry files
+void* ref_telemetry_create() { return new wake::TelemetryExporter(); }
+void ref_telemetry_destroy(void* t) { delete static_cast<wake::TelemetryExporter*>(t); }
+void ref_telemetry_record_aero(void* t, unsigned long long step, float time, float fx, float fy, float fz,
+                               float torque_z, float rho_inf, float u_inf, float area, float chord) {
+    static_cast<wake::TelemetryExporter*>(t)->record_aero(
+        {step, time, wake::compute_aerodynamic_coefficients(fx, fy, fz, torque_z, rho_inf, u_inf, area, chord)});
+}
+void ref_telemetry_record_performance(void* t, unsigned long long step, double ms, double mlups, float max_speed,
+                                      float mass, float ke) {
+    wake::PerformanceMetric p;
+    p.step = step;
+    p.step_time_ms = ms;
+    p.mlups = mlups;
+    p.max_speed = max_speed;
+    p.total_mass = mass;
+    p.kinetic_energy = ke;
+    static_cast<wake::TelemetryExporter*>(t)->record_performance(p);
+}
+int ref_telemetry_write(void* t, int which, const char* path, const char* name, float st, float freq) {
+    auto* e = static_cast<wake::TelemetryExporter*>(t);
+    if (which == 0) return e->write_aero_csv(path) ? 0 : -1;
+    if (which == 1) return e->write_performance_csv(path) ? 0 : -1;
+    return e->write_summary_json(path, name, st, freq) ? 0 : -1;
+}
+
 float ref_strouhal_frequency(const float* signal, int n, float dt) {
     wake::StrouhalAnalyzer a;
     std::vector<float> s(signal, signal + n);

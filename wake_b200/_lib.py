@@ -134,6 +134,17 @@ _PROTOS = {
     "wake_batch_synchronize": (I, [vp]),
     "wake_batch_info": (I, [vp, vp, vp, vp, vp]),
     "wake_batch_autotune": (I, [vp, I, vp]),
+    "wake_telemetry_create": (vp, []),
+    "wake_telemetry_destroy": (None, [vp]),
+    "wake_telemetry_clear": (None, [vp]),
+    "wake_telemetry_record_aero": (I, [vp, C.c_ulonglong, F, F, F, F, F, F, F, F, F]),
+    "wake_telemetry_record_history": (I, [vp, vp, I, LL, I, I, F, F, F, F]),
+    "wake_telemetry_record_performance": (I, [vp, C.c_ulonglong, D, D, F, F, F]),
+    "wake_telemetry_count": (I, [vp, I]),
+    "wake_telemetry_get_coefficients": (I, [vp, I, vp]),
+    "wake_telemetry_write_aero_csv": (I, [vp, C.c_char_p]),
+    "wake_telemetry_write_performance_csv": (I, [vp, C.c_char_p]),
+    "wake_telemetry_write_summary_json": (I, [vp, C.c_char_p, C.c_char_p, F, F]),
     "wake_strouhal_frequency": (D, [vp, I, D]),
 }
 

@@ -85,7 +85,8 @@ class ServeReport:
     def summary(self) -> dict:
         lat = np.array([r.latency for r in self.results]) if self.results else np.zeros(1)
         done = [r for r in self.results if r.error is None]
-        return {"jobs": len(self.results), "failed": len(self.results) - len(done),
+        failed = [[r.id, r.kind, (r.error or "")[:160]] for r in self.results if r.error is not None]
+        return {"jobs": len(self.results), "failed": len(failed), "failed_jobs": failed[:10],
                 "sims_per_s": len(self.results) / self.makespan if self.makespan > 0 else 0.0,
                 "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
                 "mean_latency_s": float(lat.mean()), "makespan_s": self.makespan, "ticks": self.ticks,
