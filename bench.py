@@ -50,6 +50,9 @@ def parse():
     p.add_argument("--no-batch", action="store_true", help="skip the batched ellipse-sweep leg")
     p.add_argument("--batch-only", action="store_true", help="only the batched ellipse-sweep leg (one JSON line)")
     p.add_argument("--no-serve", action="store_true", help="skip the served-mix leg")
+    p.add_argument("--no-tgv", action="store_true", help="skip the D3Q27 MRT Taylor-Green 384^3 leg")
+    p.add_argument("--tgv-steps", type=int, default=5000, help="steps of the Taylor-Green leg (multiple of 500)")
+    p.add_argument("--tgv-only", action="store_true", help="only the Taylor-Green leg (one JSON line)")
     p.add_argument("--serve-rate", type=float, default=20.0, help="arrival rate of the served-mix leg (jobs/s)")
     p.add_argument("--serve-jobs", type=int, default=60, help="jobs in the served-mix leg")
     p.add_argument("--serve-graph", type=int, default=20, help="steps per CUDA graph inside a served batch (0: plain)")
@@ -346,6 +349,106 @@ def serving_leg(rate, n_jobs, storage="f32", baseline=True, graph_steps=20):
     return out
 
 
+TGV_WORKLOAD = ("D3Q27 MRT periodic Taylor-Green vortex 384^3, u0=0.04, tau=0.51, FP32 populations vs FP16 and "
+                "BF16 shifted storage (FP32 arithmetic)")
+
+
+def tgv_leg(L=384, steps=5000, every=500, graph=20):
+    """The three storages of the Taylor-Green lattice advanced side by side in chunks of `every` steps.
+
+    Per chunk and storage: CUDA-event time of the chunk (the first chunk is warm-up and untimed),
+    FP64 kinetic energy, and the velocity relative L2 error of FP16/BF16 against FP32 at the same
+    step. KE is also set against the linear viscous decay exp(-6 nu k^2 t) of this initial field
+    (its Laplacian is -3 k^2 u); the vortex is nonlinear at Re = u0/(nu k) = 733, so that column is
+    context, not a gate. The FP64-oracle comparison runs at 32^3 in the tests."""
+    import torch
+
+    import wake_b200 as wb
+    from wake_b200 import workloads as W
+
+    u0, tau = 0.04, 0.51
+    n = L ** 3
+    fields = W.taylor_green_fields_device(L, u0)
+    stream = torch.cuda.Stream()
+    grids = {}
+    for st in ("f32", "f16", "bf16"):
+        g = wb.LatticeGrid3DQ27(L, L, L, tau, storage=st)
+        g.set_stream(stream.cuda_stream)
+        g.initialize_fields(*fields)
+        g.set_periodic_axes(True, True)
+        if graph:
+            g.use_graph(graph)
+        grids[st] = g
+    del fields
+    nu = (tau - 0.5) / 3.0
+    k = 2.0 * math.pi / L
+    ke0 = {st: g.compute_total_kinetic_energy() for st, g in grids.items()}
+    u = {st: torch.empty((3, n), dtype=torch.float32, device="cuda") for st in grids}
+    ms = {st: 0.0 for st in grids}
+    timed_steps_done = 0
+    rows = []
+    for c in range(steps // every):
+        for st, g in grids.items():
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g.step(wb.MRT, n=every)
+            e1.record(stream)
+            e1.synchronize()
+            if c > 0:
+                ms[st] += e0.elapsed_time(e1)
+            g.synchronize()
+            g.macroscopic_into(ux=u[st][0], uy=u[st][1], uz=u[st][2])
+        if c > 0:
+            timed_steps_done += every
+        t = (c + 1) * every
+        ref_norm = torch.linalg.vector_norm(u["f32"].double()).item()
+        row = {"step": t, "ke_ratio_linear": math.exp(-6.0 * nu * k * k * t)}
+        for st, g in grids.items():
+            row[f"ke_ratio_{st}"] = g.compute_total_kinetic_energy() / ke0[st]
+            if st != "f32":
+                row[f"u_rel_l2_{st}_vs_f32"] = torch.linalg.vector_norm((u[st] - u["f32"]).double()).item() / ref_norm
+        rows.append(row)
+    out = {"workload": TGV_WORKLOAD, "nodes": n, "steps": steps, "timed_steps": timed_steps_done,
+           "graph_steps": graph, "checkpoints": rows}
+    peak, _ = hbm_peak()
+    for st in grids:
+        bpn = 2 * 27 * (4 if st == "f32" else 2) + 1
+        sec = ms[st] * 1e-3
+        mlups = n * timed_steps_done / sec / 1e6 if sec > 0 else None
+        gbs = bpn * n * timed_steps_done / sec / 1e9 if sec > 0 else None
+        out[st] = {"mlups": mlups, "ms_per_step": ms[st] / max(1, timed_steps_done), "bytes_per_node": bpn,
+                   "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peak if gbs else None}
+    if out["f32"]["mlups"]:
+        for st in ("f16", "bf16"):
+            out[st]["speedup_vs_f32"] = out[st]["mlups"] / out["f32"]["mlups"]
+    for g in grids.values():
+        g.close()
+    # vorticity + Q-criterion of the final FP32 velocity: the drop-in kernel with device buffers,
+    # 12 B read + 16 B written per node; CUDA events around each call on the legacy stream it uses
+    res = torch.empty((4, n), dtype=torch.float32, device="cuda")
+    uf = u["f32"]
+    ev = []
+    for i in range(13):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(torch.cuda.default_stream())
+        wb.lib.compute_vorticity_and_q_criterion_3d(uf[0].data_ptr(), uf[1].data_ptr(), uf[2].data_ptr(),
+                                                    res[0].data_ptr(), res[1].data_ptr(), res[2].data_ptr(),
+                                                    res[3].data_ptr(), L, L, L)
+        e1.record(torch.cuda.default_stream())
+        e1.synchronize()
+        if i >= 3:
+            ev.append(e0.elapsed_time(e1))
+    ms_q = statistics.median(ev)
+    out["vorticity_q"] = {"ms_per_call": ms_q, "bytes_per_node": 28, "achieved_gbs": 28 * n / (ms_q * 1e-3) / 1e9,
+                          "frac_of_measured_hbm": 28 * n / (ms_q * 1e-3) / 1e9 / peak,
+                          "timing": "median of 10 calls after 3, CUDA events around each synchronous call "
+                                    "(includes the call's host overhead)"}
+    del res, u
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
+
+
 def reference_sample(case_ref, steps_cap, budget_s, threads=1):
     """Time the reference's own LatticeGrid3D::step + momentum exchange (oracle/_ref) on host cores."""
     import oracle
@@ -427,6 +530,9 @@ def main():
         for rate in [float(r) for r in args.serve_sweep.split(",")]:
             print(json.dumps({"workload": SERVE_WORKLOAD, **serving_leg(rate, args.serve_jobs,
                                                                           graph_steps=args.serve_graph)}), flush=True)
+        return
+    if args.tgv_only:
+        print(json.dumps(tgv_leg(steps=args.tgv_steps)))
         return
     if args.batch_only:
         out = {"workload": BATCH_WORKLOAD, "f32": batched_leg("f32"), "f16": batched_leg("f16")}
@@ -518,6 +624,9 @@ def main():
     batched = None
     if not args.no_batch:
         batched = {"workload": BATCH_WORKLOAD, "f32": batched_leg("f32"), "f16": batched_leg("f16")}
+    tgv = None
+    if not args.no_tgv:
+        tgv = tgv_leg(steps=args.tgv_steps)
     served = None
     if not args.no_serve:
         served = {"workload": SERVE_WORKLOAD, **serving_leg(args.serve_rate, args.serve_jobs)}
@@ -540,7 +649,7 @@ def main():
                            "l2": "inputs larger than L2 (two 319 MB population buffers, 126 MB L2)",
                            "parallelism": "replicas" if world > 1 else "single GPU",
                            "graph_steps": args.graph, "final_cd": cd},
-                "roofline": roof, "fp16": fp16, "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "served": served,
+                "roofline": roof, "fp16": fp16, "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "taylor_green": tgv, "served": served,
                 "clocks": clocks.summary(),
                 "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line))

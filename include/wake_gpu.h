@@ -150,6 +150,15 @@ void thermal_compute_buoyancy_force_2d(const float temperature[], float gy_body[
                                        float g_gravity, int count);
 void thermal_apply_isothermal_wall(float g[], int nx, int ny, int y_wall, float t_wall);
 
+/* Field analytics: src/ispc/analytics_kernels.ispc:4-10 (2D vorticity), 33-44
+ * (3D vorticity vector + Q-criterion). Central differences with periodic wrap;
+ * products and sums rounded in the reference's order without contraction.
+ * Called by FieldAnalytics (src/analytics/field_analytics.cpp:5-14). */
+void compute_vorticity_2d(const float ux[], const float uy[], float vorticity[], int nx, int ny);
+void compute_vorticity_and_q_criterion_3d(const float ux[], const float uy[], const float uz[], float omega_x[],
+                                          float omega_y[], float omega_z[], float q_criterion[], int nx, int ny,
+                                          int nz);
+
 /* ---------------------------------------------------------- fused engine */
 typedef struct wake_grid wake_grid;
 
@@ -353,6 +362,38 @@ int wake_batch_info(wake_batch* b, long long* nodes, int* bulk_rows, int* genera
 /* Times `steps` real steps per bulk block size (64, 128, 256) and keeps the
  * fastest; members advance 3 * steps. Results do not depend on the choice. */
 int wake_batch_autotune(wake_batch* b, int steps, int* best_threads);
+
+/* ------------------------------------------------------------------ field analytics and VTK
+ * FieldAnalytics (src/analytics/field_analytics.cpp:18-63) on the device, from
+ * the moments of the grid's current state (the same ux/uy/uz the reference
+ * passes from grid.ux_data()): 2D vorticity, 3D vorticity vector + Q-criterion,
+ * and the largest |vorticity| in 2D. Outputs are host or device memory, one
+ * float per node. wake_field_abs_max = compute_max_vorticity_2d on any float
+ * array (host or device; NaN values are skipped, as std::max from 0 does). */
+int wake_grid_compute_vorticity(wake_grid* g, float* vorticity);
+int wake_grid_compute_3d_features(wake_grid* g, float* omega_x, float* omega_y, float* omega_z, float* q_criterion);
+int wake_grid_max_vorticity(wake_grid* g, float* max_vorticity);
+int wake_field_abs_max(const float* values, long long count, float* max_abs);
+
+/* VTK XML ImageData (.vti, ASCII) and ParaView .pvd collections in the bytes
+ * wake::VtkExporter writes (src/export/vtk_exporter.cpp:8-223) for the same
+ * fields: Velocity, Speed, Density, then Vorticity (2D) or Q_Criterion and
+ * Vorticity (3D) when given, then CellType. Arrays are host memory, x fastest;
+ * vorticity_x/y/z are the three components as separate arrays (written
+ * interleaved, as the reference's Vec3 array). Formatting runs on `threads`
+ * host threads (<= 0: all cores) and gives the same bytes for any count.
+ * wake_grid_export_vti writes a grid's current state (moments, cell types and,
+ * when `analytics` is nonzero, the device-computed vorticity / Q-criterion).
+ * Return 0, or WAKE_ERR_INVALID when the file cannot be written. */
+int wake_vtk_write_vti_2d(const char* path, int nx, int ny, const float* ux, const float* uy, const float* speed,
+                          const float* rho, const float* vorticity, const uint8_t* cell_type, int threads);
+int wake_vtk_write_vti_3d(const char* path, int nx, int ny, int nz, const float* ux, const float* uy,
+                          const float* uz, const float* speed, const float* rho, const float* q_criterion,
+                          const float* vorticity_x, const float* vorticity_y, const float* vorticity_z,
+                          const uint8_t* cell_type, int threads);
+int wake_vtk_write_pvd(const char* manifest_path, const char* file_prefix, int start_step, int end_step,
+                       int step_interval, float dt);
+int wake_grid_export_vti(wake_grid* g, const char* path, int analytics, int threads);
 
 /* ------------------------------------------------------------------ telemetry files
  * The reference's telemetry formats (wake::TelemetryExporter,

@@ -119,6 +119,10 @@ def ref() -> C.CDLL | None:
             "ref3d_get_cell_types": (None, [vp, vp]), "ref3d_num_links": (I, [vp]),
             "ref3d_get_links": (None, [vp, vp, vp, vp]), "ref3d_is_periodic": (I, [vp]),
             "ref3d_total_mass": (F, [vp]), "ref_strouhal_frequency": (F, [vp, I, F]),
+            "ref_vtk_export_2d": (I, [vp, C.c_char_p, vp]), "ref_vtk_export_3d": (I, [vp, C.c_char_p, vp, vp]),
+            "ref_vtk_pvd": (I, [C.c_char_p, C.c_char_p, I, I, I, F]),
+            "compute_vorticity_2d": (None, [vp, vp, vp, I, I]),
+            "compute_vorticity_and_q_criterion_3d": (None, [vp, vp, vp, vp, vp, vp, vp, I, I, I]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -224,6 +228,42 @@ def equilibrium(q: int, rho, ux, uy, uz=None, prec: int = 32) -> np.ndarray:
 def strouhal_frequency(signal, dt=1.0) -> float:
     s = np.ascontiguousarray(signal, np.float64)
     return float(lib().og_strouhal_frequency(_addr(s), len(s), dt))
+
+
+def vorticity_2d(ux, uy, nx: int, ny: int, dtype=np.float32) -> np.ndarray:
+    """omega_z = 0.5 (uy[x+1] - uy[x-1]) - 0.5 (ux[y+1] - ux[y-1]), periodic wrap
+    (src/ispc/analytics_kernels.ispc:4-29). Each operation rounds to `dtype`, in the
+    reference's order (float32: the reference expression evaluated without contraction)."""
+    t = np.dtype(dtype).type
+    ux = np.asarray(ux, dtype).reshape(ny, nx)
+    uy = np.asarray(uy, dtype).reshape(ny, nx)
+    h = t(0.5)
+    duy_dx = h * (np.roll(uy, -1, axis=1) - np.roll(uy, 1, axis=1))
+    dux_dy = h * (np.roll(ux, -1, axis=0) - np.roll(ux, 1, axis=0))
+    return (duy_dx - dux_dy).ravel()
+
+
+def vorticity_q_3d(ux, uy, uz, nx: int, ny: int, nz: int, dtype=np.float32):
+    """Vorticity vector and Q = 0.5 (|Omega|^2 - |S|^2) by central differences with
+    periodic wrap (src/ispc/analytics_kernels.ispc:31-110), every operation rounded
+    to `dtype` in the reference's order. Returns (omega_x, omega_y, omega_z, Q)."""
+    t = np.dtype(dtype).type
+    u = [np.asarray(a, dtype).reshape(nz, ny, nx) for a in (ux, uy, uz)]
+    h, two = t(0.5), t(2.0)
+
+    def d(a, axis):  # axis 2 = x, 1 = y, 0 = z
+        return h * (np.roll(a, -1, axis=axis) - np.roll(a, 1, axis=axis))
+
+    dux_dx, dux_dy, dux_dz = d(u[0], 2), d(u[0], 1), d(u[0], 0)
+    duy_dx, duy_dy, duy_dz = d(u[1], 2), d(u[1], 1), d(u[1], 0)
+    duz_dx, duz_dy, duz_dz = d(u[2], 2), d(u[2], 1), d(u[2], 0)
+    wx, wy, wz = duz_dy - duy_dz, dux_dz - duz_dx, duy_dx - dux_dy
+    s_xy, s_yz, s_xz = h * (dux_dy + duy_dx), h * (duy_dz + duz_dy), h * (dux_dz + duz_dx)
+    norm_s = ((dux_dx * dux_dx + duy_dy * duy_dy) + duz_dz * duz_dz) + two * ((s_xy * s_xy + s_yz * s_yz) + s_xz * s_xz)
+    o_xy, o_yz, o_xz = h * (dux_dy - duy_dx), h * (duy_dz - duz_dy), h * (dux_dz - duz_dx)
+    norm_o = two * ((o_xy * o_xy + o_yz * o_yz) + o_xz * o_xz)
+    q = h * (norm_o - norm_s)
+    return wx.ravel(), wy.ravel(), wz.ravel(), q.ravel()
 
 
 def d3q19_minv(rounded: bool) -> np.ndarray:

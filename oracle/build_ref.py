@@ -17,7 +17,7 @@ The translated files are written to ``oracle/_ref/gen`` and compiled with g++
 sources with the reference's own C++ flags, -O3 -pthread)
 together with the reference's host C++ compiled from where it lies
 (src/grid/lattice_grid_2d.cpp, src/grid/lattice_grid_3d.cpp, src/core/memory.cpp,
-src/forces/strouhal_analyzer.cpp, src/export/csv_telemetry.cpp)
+src/forces/strouhal_analyzer.cpp, src/export/csv_telemetry.cpp, src/export/vtk_exporter.cpp)
 and the thin extern "C" shim ``oracle/ref_shim.cpp``. The output is
 ``oracle/_ref/libwake_ref.so``. Nothing is copied into the repository: the
 output directory is git-ignored.
@@ -79,7 +79,8 @@ def build(verbose: bool = False) -> Path:
             ref / "src" / "grid" / "lattice_grid_3d.cpp",
             ref / "src" / "core" / "memory.cpp",
             ref / "src" / "forces" / "strouhal_analyzer.cpp",
-            ref / "src" / "export" / "csv_telemetry.cpp"]
+            ref / "src" / "export" / "csv_telemetry.cpp",
+            ref / "src" / "export" / "vtk_exporter.cpp"]
     so = OUT / "libwake_ref.so"
     # the translated kernels with ISPC's fast-math avx2 settings (CMakeLists.txt:24), the
     # host sources with the reference's C++ flags (CMakeLists.txt:25)

@@ -1,7 +1,8 @@
 // extern "C" shim over the reference's own host classes (test infrastructure only).
 //
 // Compiled by oracle/build_ref.py together with the reference sources
-// (src/grid/lattice_grid_{2d,3d}.cpp, src/forces/strouhal_analyzer.cpp) and the
+// (src/grid/lattice_grid_{2d,3d}.cpp, src/forces/strouhal_analyzer.cpp,
+// src/export/csv_telemetry.cpp, src/export/vtk_exporter.cpp) and the
 // mechanically translated ISPC kernels. It lets the Python tests drive
 // wake::LatticeGrid2D / wake::LatticeGrid3D exactly as the reference scenarios do
 // (src/scenarios/karman_vortex.cpp:62-124, src/scenarios/sphere_3d_wake.cpp:64-105)
@@ -17,6 +18,7 @@
 #undef private
 #include "wake/forces/strouhal_analyzer.hpp"
 #include "wake/export/csv_telemetry.hpp"
+#include "wake/export/vtk_exporter.hpp"
 
 namespace ispc {
 extern "C" {
@@ -202,6 +204,25 @@ int ref_telemetry_write(void* t, int which, const char* path, const char* name, 
     if (which == 0) return e->write_aero_csv(path) ? 0 : -1;
     if (which == 1) return e->write_performance_csv(path) ? 0 : -1;
     return e->write_summary_json(path, name, st, freq) ? 0 : -1;
+}
+
+// ---------------------------------------------------------------- VTK files
+int ref_vtk_export_2d(void* h, const char* path, const float* vorticity) {
+    return wake::VtkExporter::export_vti_2d(path, *static_cast<LatticeGrid2D*>(h), vorticity) ? 0 : -1;
+}
+// vorticity: n interleaved (x, y, z) triples, or NULL
+int ref_vtk_export_3d(void* h, const char* path, const float* q_criterion, const float* vorticity) {
+    auto* g = static_cast<LatticeGrid3D*>(h);
+    std::vector<wake::Vec3> v;
+    if (vorticity) {
+        const std::size_t n = g->total_nodes();
+        v.resize(n);
+        for (std::size_t i = 0; i < n; ++i) v[i] = wake::Vec3(vorticity[3 * i], vorticity[3 * i + 1], vorticity[3 * i + 2]);
+    }
+    return wake::VtkExporter::export_vti_3d(path, *g, q_criterion, vorticity ? v.data() : nullptr) ? 0 : -1;
+}
+int ref_vtk_pvd(const char* path, const char* prefix, int start, int end, int interval, float dt) {
+    return wake::VtkExporter::write_pvd_manifest(path, prefix, start, end, interval, dt) ? 0 : -1;
 }
 
 float ref_strouhal_frequency(const float* signal, int n, float dt) {

@@ -199,3 +199,35 @@ def test_batch_rejects_mismatched_members():
         b.step(1)
     b.close()
     g3.close()
+
+
+@pytest.mark.parametrize("graph", [0, 10])
+def test_member_replaced_at_the_same_address_gets_its_own_rows(graph):
+    """A batch whose only member finished and was destroyed takes a new grid, which the host
+    allocator may place at the destroyed grid's address, with an equally new geometry. The batch
+    must rebuild its row lists for the newcomer (the newcomer is larger, so stale lists would
+    leave rows unstepped rather than reach past a buffer)."""
+    small, big = sorted(_sweep(8), key=lambda c: c.n)[0], sorted(_sweep(8), key=lambda c: c.n)[-1]
+    assert big.n > small.n
+    steps = 24
+    b = Batch(9, "f32")
+    if graph:
+        b.use_graph(graph)
+    reused = 0
+    for _ in range(3):
+        g = W.build_grid(small)
+        _add(b, g, small)
+        b.step(steps)
+        old = g.handle
+        b.remove(g)
+        g.close()
+        g = W.build_grid(big)
+        reused += int(g.handle == old)
+        _add(b, g, big)
+        b.step(steps)
+        snap = _snapshot(g)
+        b.remove(g)
+        g.close()
+        _same(snap, _alone(big, steps))
+    print(f"[batch] newcomer reused the destroyed grid's address in {reused} of 3 rounds")
+    b.close()

@@ -5,12 +5,13 @@ ABI of include/wake_gpu.h). This package is a thin Python mirror of the
 reference's host classes over that ABI; it never computes on the CPU.
 """
 from ._lib import EXPORTED, LIB_PATH, WakeError, addr, check, lib
+from .analytics import FieldAnalytics, VtkExporter
 from .grid import (BGK, FLUID, INFLOW, MOVING_WALL, MRT, OUTFLOW, SOLID, TRT, LatticeGrid2D, LatticeGrid3D,
                    LatticeGrid3DQ27)
 
 __all__ = [
     "lib", "check", "addr", "WakeError", "EXPORTED", "LIB_PATH",
-    "LatticeGrid2D", "LatticeGrid3D", "LatticeGrid3DQ27",
+    "LatticeGrid2D", "LatticeGrid3D", "LatticeGrid3DQ27", "FieldAnalytics", "VtkExporter",
     "BGK", "TRT", "MRT", "FLUID", "SOLID", "INFLOW", "OUTFLOW", "MOVING_WALL",
 ]
 

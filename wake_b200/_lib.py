@@ -67,6 +67,8 @@ _PROTOS = {
     "thermal_collide_d2q9": (None, [vp, vp, vp, vp, vp, vp, F, I]),
     "thermal_compute_buoyancy_force_2d": (None, [vp, vp, F, F, F, I]),
     "thermal_apply_isothermal_wall": (None, [vp, I, I, I, F]),
+    "compute_vorticity_2d": (None, [vp, vp, vp, I, I]),
+    "compute_vorticity_and_q_criterion_3d": (None, [vp, vp, vp, vp, vp, vp, vp, I, I, I]),
     # fused engine
     "wake_grid_create": (vp, [I, I, I, I, F, I]),
     "wake_grid_destroy": (None, [vp]),
@@ -134,6 +136,14 @@ _PROTOS = {
     "wake_batch_synchronize": (I, [vp]),
     "wake_batch_info": (I, [vp, vp, vp, vp, vp]),
     "wake_batch_autotune": (I, [vp, I, vp]),
+    "wake_grid_compute_vorticity": (I, [vp, vp]),
+    "wake_grid_compute_3d_features": (I, [vp, vp, vp, vp, vp]),
+    "wake_grid_max_vorticity": (I, [vp, vp]),
+    "wake_field_abs_max": (I, [vp, LL, vp]),
+    "wake_vtk_write_vti_2d": (I, [C.c_char_p, I, I, vp, vp, vp, vp, vp, vp, I]),
+    "wake_vtk_write_vti_3d": (I, [C.c_char_p, I, I, I, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, I]),
+    "wake_vtk_write_pvd": (I, [C.c_char_p, C.c_char_p, I, I, I, F]),
+    "wake_grid_export_vti": (I, [vp, C.c_char_p, I, I]),
     "wake_telemetry_create": (vp, []),
     "wake_telemetry_destroy": (None, [vp]),
     "wake_telemetry_clear": (None, [vp]),

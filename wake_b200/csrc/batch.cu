@@ -61,7 +61,7 @@ struct wake_batch {
     int parity = 0;  // batch steps taken, mod 2
 
     // row lists are rebuilt when the members or any member's geometry change
-    std::vector<std::pair<const wake_grid*, unsigned>> layout;
+    std::vector<std::pair<const wake_grid*, unsigned long long>> layout;
     std::vector<int> gen_first;
     unsigned shape = 0;  // bumped when launch shapes or table addresses change
 
@@ -106,7 +106,7 @@ bool valid_batch(wake_batch* b) {
 
 // Rebuild the concatenated row lists when the membership or a member's geometry changed.
 int build_rows(wake_batch* b) {
-    std::vector<std::pair<const wake_grid*, unsigned>> layout;
+    std::vector<std::pair<const wake_grid*, unsigned long long>> layout;
     layout.reserve(b->members.size());
     for (const auto& m : b->members) layout.emplace_back(m.g, m.g->geom_version);
     if (layout == b->layout && b->gen_first.size() == b->members.size()) return WAKE_OK;

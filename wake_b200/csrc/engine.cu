@@ -7,12 +7,14 @@
 // is where the work happens: the state lives in HBM as two SoA population
 // buffers and one step is one kernel launch (stream_collide.cuh).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <numeric>
 #include <string>
 #include <vector>
 
+#include "analytics.cuh"
 #include "engine.cuh"
 
 namespace wk {
@@ -21,6 +23,11 @@ namespace {
 thread_local std::string t_err;
 thread_local int t_code = 0;
 }  // namespace
+
+unsigned long long next_geom_version() {
+    static std::atomic<unsigned long long> counter{0};
+    return ++counter;
+}
 
 int set_error(int code, const std::string& msg) {
     t_err = msg;
@@ -415,7 +422,7 @@ int rebuild_flags(wake_grid* g) {
         g->h_fast_rows = std::move(spans);
         g->h_gen_rows = std::move(gen);
     }
-    ++g->geom_version;
+    g->geom_version = next_geom_version();
     g->geom_dirty = false;
     g->invalidate_graph();
     return WAKE_OK;
@@ -1406,6 +1413,112 @@ int wake_grid_diagnostics(wake_grid* g, double* total_mass, double* kinetic_ener
     return WAKE_OK;
 }
 
+// ---------------------------------------------------------------- field analytics
+// FieldAnalytics::compute_vorticity / compute_3d_features / compute_max_vorticity_2d
+// (src/analytics/field_analytics.cpp:18-63) on the device, from the moments of
+// the current state. Outputs may be host or device memory (one float per node).
+static bool on_device(const void* p) {
+    cudaPointerAttributes a{};
+    const cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int wake_grid_compute_vorticity(wake_grid* g, float* vorticity) {
+    if (!valid_grid(g) || !vorticity) return set_error(WAKE_ERR_INVALID, "null vorticity output");
+    if (g->D != 2) return set_error(WAKE_ERR_INVALID, "wake_grid_compute_vorticity: D2Q9 lattices only");
+    int r = apply_geometry(g);
+    if (r) return r;
+    r = materialise(g, false, true);
+    if (r) return r;
+    const std::size_t b = sizeof(float) * g->N;
+    float* out = vorticity;
+    if (!on_device(vorticity)) {
+        WK_CUDA(g->m_an.ensure(b));
+        out = g->m_an.as<float>();
+    }
+    k_vorticity_2d<<<analytics_grid_3d(g->nx, g->ny, 1, 128), 128, 0, g->stream>>>(
+        g->m_ux.as<float>(), g->m_uy.as<float>(), out, g->nx, g->ny);
+    WK_CUDA(cudaGetLastError());
+    if (out != vorticity) WK_CUDA(cudaMemcpyAsync(vorticity, out, b, cudaMemcpyDeviceToHost, g->stream));
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    return WAKE_OK;
+}
+
+int wake_grid_compute_3d_features(wake_grid* g, float* omega_x, float* omega_y, float* omega_z, float* q_criterion) {
+    if (!valid_grid(g) || !omega_x || !omega_y || !omega_z || !q_criterion)
+        return set_error(WAKE_ERR_INVALID, "null vorticity or Q-criterion output");
+    if (g->D != 3) return set_error(WAKE_ERR_INVALID, "wake_grid_compute_3d_features: 3D lattices only");
+    int r = apply_geometry(g);
+    if (r) return r;
+    r = materialise(g, false, true);
+    if (r) return r;
+    const std::size_t b = sizeof(float) * g->N;
+    float* user[4] = {omega_x, omega_y, omega_z, q_criterion};
+    float* out[4];
+    bool staged = false;
+    for (int i = 0; i < 4; ++i) staged = staged || !on_device(user[i]);
+    if (staged) WK_CUDA(g->m_an.ensure(4 * b));
+    for (int i = 0; i < 4; ++i) out[i] = on_device(user[i]) ? user[i] : g->m_an.as<float>() + i * g->N;
+    k_vorticity_q_3d<<<analytics_grid_3d(g->nx, g->ny, g->nz, 128), 128, 0, g->stream>>>(
+        g->m_ux.as<float>(), g->m_uy.as<float>(), g->m_uz.as<float>(), out[0], out[1], out[2], out[3], g->nx, g->ny,
+        g->nz);
+    WK_CUDA(cudaGetLastError());
+    for (int i = 0; i < 4; ++i)
+        if (out[i] != user[i]) WK_CUDA(cudaMemcpyAsync(user[i], out[i], b, cudaMemcpyDeviceToHost, g->stream));
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    return WAKE_OK;
+}
+
+// Largest |v| of device values on `stream` (k_absmax), synchronous.
+static int abs_max_device(const float* values, long long count, float* out, cudaStream_t stream, DevMem& word) {
+    WK_CUDA(word.ensure(sizeof(unsigned)));
+    WK_CUDA(cudaMemsetAsync(word.p, 0, sizeof(unsigned), stream));
+    if (count > 0) {
+        const long long want = (count + 255) / 256;
+        const int blocks = static_cast<int>(want < 148 * 8 ? want : 148 * 8);
+        k_absmax<<<blocks, 256, 0, stream>>>(values, count, word.as<unsigned>());
+        WK_CUDA(cudaGetLastError());
+    }
+    unsigned bits = 0;
+    WK_CUDA(cudaMemcpyAsync(&bits, word.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    WK_CUDA(cudaStreamSynchronize(stream));
+    std::memcpy(out, &bits, sizeof(float));
+    return WAKE_OK;
+}
+
+int wake_grid_max_vorticity(wake_grid* g, float* max_vorticity) {
+    if (!valid_grid(g) || !max_vorticity) return set_error(WAKE_ERR_INVALID, "null output");
+    if (g->D != 2) return set_error(WAKE_ERR_INVALID, "wake_grid_max_vorticity: D2Q9 lattices only");
+    const std::size_t b = sizeof(float) * g->N;
+    WK_CUDA(g->m_an.ensure(b));
+    float* v = g->m_an.as<float>();
+    const int r = wake_grid_compute_vorticity(g, v);
+    if (r) return r;
+    DevMem word;
+    return abs_max_device(v, static_cast<long long>(g->N), max_vorticity, g->stream, word);
+}
+
+int wake_field_abs_max(const float* values, long long count, float* out) {
+    if (!out || count < 0 || (!values && count > 0))
+        return set_error(WAKE_ERR_INVALID, "wake_field_abs_max: bad argument");
+    if (count == 0) {
+        *out = 0.0f;
+        return WAKE_OK;
+    }
+    DevMem staged, word;
+    const float* v = values;
+    if (!on_device(values)) {
+        WK_CUDA(staged.ensure(sizeof(float) * static_cast<std::size_t>(count)));
+        WK_CUDA(cudaMemcpy(staged.p, values, sizeof(float) * static_cast<std::size_t>(count), cudaMemcpyHostToDevice));
+        v = staged.as<float>();
+    }
+    return abs_max_device(v, count, out, nullptr, word);
+}
+
 int wake_grid_total_mass(wake_grid* g, double* mass) {
     if (!valid_grid(g) || !mass) return set_error(WAKE_ERR_INVALID, "null output");
     double d[4];
@@ -1432,7 +1545,7 @@ long long wake_grid_device_bytes(wake_grid* g) {
                            &g->d_link_q, &g->d_link_delta, &g->d_link_mom, &g->d_counters, &g->d_hist,
                            &g->d_warp_base, &g->d_contrib, &g->d_fast_rows, &g->d_gen_rows, &g->m_f, &g->m_rho,
                            &g->m_ux, &g->m_uy, &g->m_uz, &g->m_speed, &g->m_diag, &g->TA, &g->TB, &g->m_t,
-                           &g->d_tiles, &g->d_gen4, &g->d_mixed};
+                           &g->d_tiles, &g->d_gen4, &g->d_mixed, &g->m_an};
     long long sum = 0;
     for (const DevMem* m : all) sum += static_cast<long long>(m->bytes);
     return sum;
@@ -1465,6 +1578,7 @@ int wake_grid_release_scratch(wake_grid* g) {
         g->m_t.reset();
         g->mt_valid = false;
     }
+    g->m_an.reset();
     g->m_rho.reset();
     g->m_ux.reset();
     g->m_uy.reset();

@@ -100,7 +100,10 @@ struct wake_grid {
         for (const uint4& sp : h_fast_rows) n += sp.w - sp.z;
         return n;
     }
-    unsigned geom_version = 0;                      // bumped whenever the flags / row lists are rebuilt
+    // Identity of the current flags / row lists: a fresh process-wide number at every
+    // rebuild (next_geom_version), so a batch never takes a new grid that happens to
+    // reuse a destroyed grid's address for the old one.
+    unsigned long long geom_version = 0;
 
     int tpb = 0, xchunks = 1, rows = 1, tpb_fast = 256;
     // step kernels: 0 automatic, 1 direct (k_step_fast for the pure-gather rows beside
@@ -120,6 +123,7 @@ struct wake_grid {
     long long k = 0;
 
     DevMem m_f, m_rho, m_ux, m_uy, m_uz, m_speed, m_diag;
+    DevMem m_an;  // field analytics: vorticity (2D) or omega x/y/z + Q (3D), and the |max| word
 
     // coupled D2Q5 temperature (D2Q9 lattices): post-collision populations in TA / TB
     // (same parity as A / B), FP32 start-up populations in m_t
@@ -150,7 +154,7 @@ struct wake_grid {
             DevMem* all[] = {&A, &B, &d_types, &d_flags, &d_status, &d_nodestart, &d_link_node, &d_link_q,
                              &d_link_delta, &d_link_mom, &d_counters, &d_hist, &d_warp_base, &d_contrib,
                              &d_fast_rows, &d_gen_rows, &d_tiles, &d_gen4, &d_mixed, &m_f, &m_rho, &m_ux, &m_uy, &m_uz,
-                             &m_speed, &m_diag, &TA, &TB, &m_t};
+                             &m_speed, &m_diag, &TA, &TB, &m_t, &m_an};
             for (DevMem* m : all) m->release();
         }
         for (cudaEvent_t e : t_ev) cudaEventDestroy(e);
@@ -237,6 +241,7 @@ bool grid_valid(wake_grid* g);
 // Bring a lattice to the point where its state buffers hold Collide(f^k) for the
 // current geometry and parameters (rebuilds flags, re-collides when pending).
 int grid_prepare(wake_grid* g);
+unsigned long long next_geom_version();
 // Step arguments of one lattice (rows and buffers left for the caller).
 StepArgs grid_step_args(const wake_grid* g);
 // Bookkeeping after n steps run outside wake_grid_step (by a batch).

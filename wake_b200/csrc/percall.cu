@@ -14,6 +14,7 @@
 
 #include "common.cuh"
 #include "lattice.cuh"
+#include "analytics.cuh"
 #include "stream_collide.cuh"
 #include "wake_gpu.h"
 
@@ -44,6 +45,9 @@ class Stager {
     // entries (e.g. moments at solid nodes) untouched, and those keep the caller's values.
     template <class T>
     T* out(T* p, std::size_t n) { return static_cast<T*>(add(p, n * sizeof(T), true, true)); }
+    // An output the kernel writes in full: nothing to copy in.
+    template <class T>
+    T* full_out(T* p, std::size_t n) { return static_cast<T*>(add(p, n * sizeof(T), false, true)); }
 
     // Allocate the arena and copy staged inputs. Returns 0 or an error code.
     int begin() {
@@ -816,6 +820,40 @@ void thermal_apply_isothermal_wall(float g[], int nx, int ny, int y_wall, float 
     s.inout(g, 9 * static_cast<std::size_t>(nx) * ny);
     if (s.begin()) return;
     k_isothermal_wall<<<blocks_for(nx, 128), 128>>>(s.ptr<float>(0), nx, ny, y_wall, t_wall);
+    s.end();
+}
+
+// src/ispc/analytics_kernels.ispc:4-29
+void compute_vorticity_2d(const float ux[], const float uy[], float vorticity[], int nx, int ny) {
+    if (nx <= 0 || ny <= 0) return;
+    const std::size_t n = static_cast<std::size_t>(nx) * ny;
+    Stager s;
+    s.in(ux, n);
+    s.in(uy, n);
+    s.full_out(vorticity, n);
+    if (s.begin()) return;
+    k_vorticity_2d<<<analytics_grid_3d(nx, ny, 1, 128), 128>>>(s.ptr<float>(0), s.ptr<float>(1), s.ptr<float>(2), nx, ny);
+    s.end();
+}
+
+// src/ispc/analytics_kernels.ispc:31-110
+void compute_vorticity_and_q_criterion_3d(const float ux[], const float uy[], const float uz[], float omega_x[],
+                                          float omega_y[], float omega_z[], float q_criterion[], int nx, int ny,
+                                          int nz) {
+    if (nx <= 0 || ny <= 0 || nz <= 0) return;
+    const std::size_t n = static_cast<std::size_t>(nx) * ny * nz;
+    Stager s;
+    s.in(ux, n);
+    s.in(uy, n);
+    s.in(uz, n);
+    s.full_out(omega_x, n);
+    s.full_out(omega_y, n);
+    s.full_out(omega_z, n);
+    s.full_out(q_criterion, n);
+    if (s.begin()) return;
+    k_vorticity_q_3d<<<analytics_grid_3d(nx, ny, nz, 128), 128>>>(s.ptr<float>(0), s.ptr<float>(1), s.ptr<float>(2),
+                                                                  s.ptr<float>(3), s.ptr<float>(4), s.ptr<float>(5),
+                                                                  s.ptr<float>(6), nx, ny, nz);
     s.end();
 }
 

@@ -93,7 +93,15 @@ class _Grid:
         check(lib.wake_grid_initialize(self._h, rho_init, ux_init, uy_init, uz_init))
 
     def initialize_fields(self, rho, ux, uy, uz=None) -> None:
-        arrs = [np.ascontiguousarray(a, dtype=np.float32).ravel() if a is not None else None for a in (rho, ux, uy, uz)]
+        """Initial populations = equilibrium of the fields (numpy arrays, or contiguous float32 CUDA tensors)."""
+        def prep(a):
+            if a is None or (hasattr(a, "data_ptr") and getattr(a, "is_cuda", False)):
+                if a is not None and (a.dtype.itemsize != 4 or not a.is_contiguous() or a.numel() != self.total_nodes()):
+                    raise ValueError("device fields must be contiguous float32 tensors of one value per node")
+                return a
+            return np.ascontiguousarray(a, dtype=np.float32).ravel()
+
+        arrs = [prep(a) for a in (rho, ux, uy, uz)]
         check(lib.wake_grid_initialize_fields(self._h, *[addr(a) for a in arrs]))
 
     def set_populations(self, f) -> None:
@@ -158,6 +166,16 @@ class _Grid:
         return out
 
     macro = macroscopic
+
+    def macroscopic_into(self, rho=None, ux=None, uy=None, uz=None, speed=None) -> None:
+        """Copy the moments after the last step into caller buffers (host arrays or CUDA tensors of one
+        float32 per node); a None buffer is skipped."""
+        for a in (rho, ux, uy, uz, speed):
+            if a is not None and (a.dtype.itemsize != 4 or (a.numel() if hasattr(a, "numel") else a.size)
+                                  != self.total_nodes()):
+                raise ValueError("moment buffers hold one float32 per node")
+        check(lib.wake_grid_get_macroscopic(self._h, addr(rho), addr(ux), addr(uy),
+                                            addr(uz) if self.Q != 9 else None, addr(speed)))
 
     def rho_data(self) -> np.ndarray:
         return self.macroscopic()["rho"]

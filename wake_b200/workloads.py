@@ -329,6 +329,21 @@ def taylor_green(L=384, u0=0.04, tau=0.51, q=27, collision=2) -> Case:
                 u_ref=u0, extra={"u0": u0, "k": k})
 
 
+def taylor_green_fields_device(L=384, u0=0.04, device="cuda"):
+    """The Taylor-Green fields of ``taylor_green`` computed on the device (FP64, rounded once to
+    float32), for lattices too large to build on the host. Returns (rho, ux, uy, uz) CUDA tensors."""
+    import torch
+
+    k = 2.0 * math.pi / L
+    x = torch.arange(L, dtype=torch.float64, device=device)
+    sx, cx_, c2 = torch.sin(k * x), torch.cos(k * x), torch.cos(2 * k * x)
+    ux = (u0 * sx[None, None, :] * cx_[None, :, None] * cx_[:, None, None]).float().reshape(-1)
+    uy = (-u0 * cx_[None, None, :] * sx[None, :, None] * cx_[:, None, None]).float().reshape(-1)
+    p = (u0 * u0 / 16.0) * (c2[None, None, :] + c2[None, :, None]) * (c2[:, None, None] + 2.0)
+    rho = (1.0 + 3.0 * p).float().reshape(-1)
+    return rho.contiguous(), ux.contiguous(), uy.contiguous(), torch.zeros_like(rho)
+
+
 def build_grid(case: Case, storage: str = "f32", les_applies: bool = True):
     """Configure a wake_b200 grid for a case (initial state = equilibrium of the fields)."""
     import wake_b200 as wb
