@@ -359,8 +359,9 @@ int wake_batch_set_kernel(wake_batch* b, int variant);
 int wake_batch_step(wake_batch* b, int n);
 int wake_batch_synchronize(wake_batch* b);        /* first member error, if any */
 int wake_batch_info(wake_batch* b, long long* nodes, int* bulk_rows, int* general_rows, int* launches_per_step);
-/* Times `steps` real steps per bulk block size (64, 128, 256) and keeps the
- * fastest; members advance 3 * steps. Results do not depend on the choice. */
+/* Times `steps` real steps per bulk block size (those of 32, 64, 128, 256 within
+ * the build's bound, 64 by default) and keeps the fastest; members advance
+ * `steps` per size tried. Results do not depend on the choice. */
 int wake_batch_autotune(wake_batch* b, int steps, int* best_threads);
 
 /* ------------------------------------------------------------------ field analytics and VTK

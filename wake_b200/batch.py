@@ -89,7 +89,7 @@ class Batch:
         return check(lib.wake_batch_get_block(self._h))
 
     def autotune(self, steps: int = 20) -> int:
-        """Pick the bulk block size by timing real steps (members advance 3 * steps)."""
+        """Pick the bulk block size by timing real steps (members advance `steps` per size tried)."""
         best = ctypes.c_int()
         check(lib.wake_batch_autotune(self._h, steps, ctypes.byref(best)))
         return best.value

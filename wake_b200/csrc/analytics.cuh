@@ -7,10 +7,11 @@
 // in the reference's evaluation order, so no multiply-add is contracted and the
 // results equal a plain IEEE float32 evaluation of the same expressions.
 //
-// One thread per node; a block covers a run of one x-row, consecutive blocks
-// the neighbouring rows, so the y and z neighbours of a block are read from L1/L2
-// and DRAM sees each velocity component about once: algorithmic traffic is
-// 8 B in + 4 B out per node in 2D and 12 B in + 16 B out per node in 3D.
+// Blocks are 32 x 8 tiles of an x-y plane, so the x and y neighbours of a tile are
+// mostly read by the same block (L1). In 3D each thread marches along z through a
+// chunk of ANALYTICS_ZC planes and keeps the z-1 / z+1 values of its column in
+// registers, so DRAM sees each velocity component about once. Algorithmic traffic
+// is 8 B in + 4 B out per node in 2D and 12 B in + 16 B out per node in 3D.
 #pragma once
 
 #include <cstdint>
@@ -21,63 +22,89 @@ namespace wk {
 
 __device__ __forceinline__ float half_diff(float a, float b) { return __fmul_rn(0.5f, __fsub_rn(a, b)); }
 
-// Grids of both stencils: x-blocks in blockIdx.x, rows (y + ny*z) spread over
-// blockIdx.y and blockIdx.z (analytics_grid_3d).
-static __global__ void k_vorticity_2d(const float* __restrict__ ux, const float* __restrict__ uy, float* __restrict__ vort,
-                                      int nx, int ny) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const long long r = static_cast<long long>(blockIdx.y) + static_cast<long long>(blockIdx.z) * gridDim.y;
-    if (x >= nx || r >= ny) return;
-    const int y = static_cast<int>(r);
-    const int ym = y == 0 ? ny - 1 : y - 1, yp = y + 1 == ny ? 0 : y + 1;
+constexpr int ANALYTICS_TX = 32, ANALYTICS_TY = 8, ANALYTICS_ZC = 32;
+
+// Grid of both stencils: x tiles in blockIdx.x, y tiles strided over blockIdx.y (any ny),
+// z chunks of ANALYTICS_ZC planes in blockIdx.z (3D; 1 in 2D). Block 32 x 8.
+static __global__ void __launch_bounds__(ANALYTICS_TX * ANALYTICS_TY)
+    k_vorticity_2d(const float* __restrict__ ux, const float* __restrict__ uy, float* __restrict__ vort, int nx,
+                   int ny) {
+    const int x = blockIdx.x * ANALYTICS_TX + threadIdx.x;
+    if (x >= nx) return;
     const int xm = x == 0 ? nx - 1 : x - 1, xp = x + 1 == nx ? 0 : x + 1;
-    const long long row = static_cast<long long>(y) * nx;
-    const float duy_dx = half_diff(uy[row + xp], uy[row + xm]);
-    const float dux_dy = half_diff(ux[static_cast<long long>(yp) * nx + x], ux[static_cast<long long>(ym) * nx + x]);
-    vort[row + x] = __fsub_rn(duy_dx, dux_dy);
+    for (long long yt = blockIdx.y; yt * ANALYTICS_TY < ny; yt += gridDim.y) {
+        const long long yl = yt * ANALYTICS_TY + threadIdx.y;
+        if (yl >= ny) break;
+        const int y = static_cast<int>(yl);
+        const int ym = y == 0 ? ny - 1 : y - 1, yp = y + 1 == ny ? 0 : y + 1;
+        const long long row = static_cast<long long>(y) * nx;
+        const float duy_dx = half_diff(uy[row + xp], uy[row + xm]);
+        const float dux_dy =
+            half_diff(ux[static_cast<long long>(yp) * nx + x], ux[static_cast<long long>(ym) * nx + x]);
+        vort[row + x] = __fsub_rn(duy_dx, dux_dy);
+    }
 }
 
 __device__ __forceinline__ float sq(float a) { return __fmul_rn(a, a); }
 
-static __global__ void k_vorticity_q_3d(const float* __restrict__ ux, const float* __restrict__ uy,
-                                        const float* __restrict__ uz, float* __restrict__ ox, float* __restrict__ oy,
-                                        float* __restrict__ oz, float* __restrict__ qc, int nx, int ny, int nz) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const long long r = static_cast<long long>(blockIdx.y) + static_cast<long long>(blockIdx.z) * gridDim.y;
-    if (x >= nx || r >= static_cast<long long>(ny) * nz) return;
-    const int y = static_cast<int>(r % ny), z = static_cast<int>(r / ny);
-    const int ym = y == 0 ? ny - 1 : y - 1, yp = y + 1 == ny ? 0 : y + 1;
-    const int zm = z == 0 ? nz - 1 : z - 1, zp = z + 1 == nz ? 0 : z + 1;
+static __global__ void __launch_bounds__(ANALYTICS_TX * ANALYTICS_TY)
+    k_vorticity_q_3d(const float* __restrict__ ux, const float* __restrict__ uy, const float* __restrict__ uz,
+                     float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz, float* __restrict__ qc,
+                     int nx, int ny, int nz) {
+    const int x = blockIdx.x * ANALYTICS_TX + threadIdx.x;
+    if (x >= nx) return;
     const int xm = x == 0 ? nx - 1 : x - 1, xp = x + 1 == nx ? 0 : x + 1;
-    const long long c = r * nx;
-    const long long cyp = (static_cast<long long>(z) * ny + yp) * nx, cym = (static_cast<long long>(z) * ny + ym) * nx;
-    const long long czp = (static_cast<long long>(zp) * ny + y) * nx, czm = (static_cast<long long>(zm) * ny + y) * nx;
+    const long long plane = static_cast<long long>(nx) * ny;
+    const int z0 = static_cast<int>(blockIdx.z) * ANALYTICS_ZC;
+    const int z1 = z0 + ANALYTICS_ZC < nz ? z0 + ANALYTICS_ZC : nz;
+    for (long long yt = blockIdx.y; yt * ANALYTICS_TY < ny; yt += gridDim.y) {
+        const long long yl = yt * ANALYTICS_TY + threadIdx.y;
+        if (yl >= ny) break;
+        const int y = static_cast<int>(yl);
+        const int ym = y == 0 ? ny - 1 : y - 1, yp = y + 1 == ny ? 0 : y + 1;
+        const long long oc = static_cast<long long>(y) * nx + x;
+        const long long oym = static_cast<long long>(ym) * nx + x, oyp = static_cast<long long>(yp) * nx + x;
+        const long long ocm = static_cast<long long>(y) * nx + xm, ocp = static_cast<long long>(y) * nx + xp;
+        // the column's values at z - 1 (lo) and z (mid); z + 1 (hi) is read at each plane
+        const long long pz0 = static_cast<long long>(z0) * plane;
+        const long long pzm = static_cast<long long>(z0 == 0 ? nz - 1 : z0 - 1) * plane;
+        float lo_x = ux[pzm + oc], lo_y = uy[pzm + oc], lo_z = uz[pzm + oc];
+        float mid_x = ux[pz0 + oc], mid_y = uy[pz0 + oc], mid_z = uz[pz0 + oc];
+        for (int z = z0; z < z1; ++z) {
+            const long long pz = static_cast<long long>(z) * plane;
+            const long long pzp = static_cast<long long>(z + 1 == nz ? 0 : z + 1) * plane;
+            const float hi_x = ux[pzp + oc], hi_y = uy[pzp + oc], hi_z = uz[pzp + oc];
 
-    const float dux_dx = half_diff(ux[c + xp], ux[c + xm]);
-    const float dux_dy = half_diff(ux[cyp + x], ux[cym + x]);
-    const float dux_dz = half_diff(ux[czp + x], ux[czm + x]);
-    const float duy_dx = half_diff(uy[c + xp], uy[c + xm]);
-    const float duy_dy = half_diff(uy[cyp + x], uy[cym + x]);
-    const float duy_dz = half_diff(uy[czp + x], uy[czm + x]);
-    const float duz_dx = half_diff(uz[c + xp], uz[c + xm]);
-    const float duz_dy = half_diff(uz[cyp + x], uz[cym + x]);
-    const float duz_dz = half_diff(uz[czp + x], uz[czm + x]);
+            const float dux_dx = half_diff(ux[pz + ocp], ux[pz + ocm]);
+            const float dux_dy = half_diff(ux[pz + oyp], ux[pz + oym]);
+            const float dux_dz = half_diff(hi_x, lo_x);
+            const float duy_dx = half_diff(uy[pz + ocp], uy[pz + ocm]);
+            const float duy_dy = half_diff(uy[pz + oyp], uy[pz + oym]);
+            const float duy_dz = half_diff(hi_y, lo_y);
+            const float duz_dx = half_diff(uz[pz + ocp], uz[pz + ocm]);
+            const float duz_dy = half_diff(uz[pz + oyp], uz[pz + oym]);
+            const float duz_dz = half_diff(hi_z, lo_z);
 
-    ox[c + x] = __fsub_rn(duz_dy, duy_dz);
-    oy[c + x] = __fsub_rn(dux_dz, duz_dx);
-    oz[c + x] = __fsub_rn(duy_dx, dux_dy);
+            ox[pz + oc] = __fsub_rn(duz_dy, duy_dz);
+            oy[pz + oc] = __fsub_rn(dux_dz, duz_dx);
+            oz[pz + oc] = __fsub_rn(duy_dx, dux_dy);
 
-    // strain rate S and rotation Omega (symmetric / antisymmetric halves of grad u)
-    const float s_xy = __fmul_rn(0.5f, __fadd_rn(dux_dy, duy_dx));
-    const float s_yz = __fmul_rn(0.5f, __fadd_rn(duy_dz, duz_dy));
-    const float s_xz = __fmul_rn(0.5f, __fadd_rn(dux_dz, duz_dx));
-    const float norm_s = __fadd_rn(__fadd_rn(__fadd_rn(sq(dux_dx), sq(duy_dy)), sq(duz_dz)),
-                                   __fmul_rn(2.0f, __fadd_rn(__fadd_rn(sq(s_xy), sq(s_yz)), sq(s_xz))));
-    const float o_xy = half_diff(dux_dy, duy_dx);
-    const float o_yz = half_diff(duy_dz, duz_dy);
-    const float o_xz = half_diff(dux_dz, duz_dx);
-    const float norm_o = __fmul_rn(2.0f, __fadd_rn(__fadd_rn(sq(o_xy), sq(o_yz)), sq(o_xz)));
-    qc[c + x] = __fmul_rn(0.5f, __fsub_rn(norm_o, norm_s));
+            // strain rate S and rotation Omega (symmetric / antisymmetric halves of grad u)
+            const float s_xy = __fmul_rn(0.5f, __fadd_rn(dux_dy, duy_dx));
+            const float s_yz = __fmul_rn(0.5f, __fadd_rn(duy_dz, duz_dy));
+            const float s_xz = __fmul_rn(0.5f, __fadd_rn(dux_dz, duz_dx));
+            const float norm_s = __fadd_rn(__fadd_rn(__fadd_rn(sq(dux_dx), sq(duy_dy)), sq(duz_dz)),
+                                           __fmul_rn(2.0f, __fadd_rn(__fadd_rn(sq(s_xy), sq(s_yz)), sq(s_xz))));
+            const float o_xy = half_diff(dux_dy, duy_dx);
+            const float o_yz = half_diff(duy_dz, duz_dy);
+            const float o_xz = half_diff(dux_dz, duz_dx);
+            const float norm_o = __fmul_rn(2.0f, __fadd_rn(__fadd_rn(sq(o_xy), sq(o_yz)), sq(o_xz)));
+            qc[pz + oc] = __fmul_rn(0.5f, __fsub_rn(norm_o, norm_s));
+
+            lo_x = mid_x, lo_y = mid_y, lo_z = mid_z;
+            mid_x = hi_x, mid_y = hi_y, mid_z = hi_z;
+        }
+    }
 }
 
 // Largest |v| over n values, NaN skipped (std::max(m, |v|) from m = 0 keeps m
@@ -95,11 +122,12 @@ static __global__ void k_absmax(const float* __restrict__ v, long long n, unsign
     if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
 }
 
-inline dim3 analytics_grid_3d(int nx, int ny, int nz, int tpb) {
-    const long long rows = static_cast<long long>(ny) * nz;
-    const unsigned gy = static_cast<unsigned>(rows < 65535 ? rows : 65535);
-    const unsigned gz = static_cast<unsigned>((rows + gy - 1) / gy);
-    return dim3(static_cast<unsigned>((nx + tpb - 1) / tpb), gy, gz);
+inline dim3 analytics_grid_3d(int nx, int ny, int nz) {
+    const long long ytiles = (static_cast<long long>(ny) + ANALYTICS_TY - 1) / ANALYTICS_TY;
+    return dim3(static_cast<unsigned>((nx + ANALYTICS_TX - 1) / ANALYTICS_TX),
+                static_cast<unsigned>(ytiles < 65535 ? ytiles : 65535),
+                static_cast<unsigned>((nz + ANALYTICS_ZC - 1) / ANALYTICS_ZC));
 }
+inline dim3 analytics_block() { return dim3(ANALYTICS_TX, ANALYTICS_TY); }
 
 }  // namespace wk

@@ -364,9 +364,10 @@ int wake_batch_use_graph(wake_batch* b, int steps_per_graph) {
 
 int wake_batch_set_block(wake_batch* b, int threads_bulk, int threads_general) {
     if (!valid_batch(b)) return WAKE_ERR_INVALID;
-    if (threads_bulk < 32 || threads_bulk > 256 || threads_bulk % 32 || threads_general < 32 ||
+    if (threads_bulk < 32 || threads_bulk > WK_FAST_MAX_THREADS || threads_bulk % 32 || threads_general < 32 ||
         threads_general > 512 || threads_general % 32)
-        return set_error(WAKE_ERR_INVALID, "wake_batch_set_block: bulk 32..256, general 32..512, multiples of 32");
+        return set_error(WAKE_ERR_INVALID, "wake_batch_set_block: bulk 32..256 (at most the fast kernels' bound), "
+                                           "general 32..512, multiples of 32");
     b->tpb_fast = threads_bulk;
     b->tpb_gen = threads_general;
     b->drop_graph();
@@ -449,9 +450,10 @@ int wake_batch_info(wake_batch* b, long long* nodes, int* bulk_rows, int* genera
     return WAKE_OK;
 }
 
-// Time `steps` real steps for each bulk block size in {64, 128, 256} (plain
-// launches, CUDA events on the batch stream) and keep the fastest. The members
-// advance by 3 * steps; results do not depend on the block size.
+// Time `steps` real steps for each bulk block size of {32, 64, 128, 256} within the
+// kernels' launch bound (plain launches, CUDA events on the batch stream) and keep
+// the fastest. The members advance `steps` per size tried; results do not depend on
+// the block size.
 int wake_batch_autotune(wake_batch* b, int steps, int* best_threads) {
     if (!valid_batch(b)) return WAKE_ERR_INVALID;
     if (steps < 1) return set_error(WAKE_ERR_INVALID, "wake_batch_autotune: steps must be positive");
@@ -467,7 +469,8 @@ int wake_batch_autotune(wake_batch* b, int steps, int* best_threads) {
     const int keep = b->tpb_fast;
     int best = keep;
     float best_ms = -1.f;
-    for (int t : {64, 128, 256}) {
+    for (int t : {32, 64, 128, 256}) {
+        if (t > WK_FAST_MAX_THREADS) break;
         b->tpb_fast = t;
         cudaEventRecord(e0, b->stream);
         r = batch_steps(b, steps);

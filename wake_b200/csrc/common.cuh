@@ -6,6 +6,21 @@
 #include <cstddef>
 #include <string>
 
+// Register budget of the pure-gather step kernels (k_step_fast, k_step_fast_batch): blocks of
+// at most WK_FAST_MAX_THREADS threads, at least WK_FAST_TRT_MIN_BLOCKS (TRT, two nodes per
+// thread) or WK_FAST_OTHER_MIN_BLOCKS (BGK / MRT, one node per thread) of them resident per SM.
+// 64 x 10 gives the packed TRT form 96 registers (20 warps per SM), measured 5-7% faster on the
+// D3Q19 sphere channel than 128 registers (16 warps) and 20% faster than 80 (24 warps, spills).
+#ifndef WK_FAST_MAX_THREADS
+#define WK_FAST_MAX_THREADS 64
+#endif
+#ifndef WK_FAST_TRT_MIN_BLOCKS
+#define WK_FAST_TRT_MIN_BLOCKS 10
+#endif
+#ifndef WK_FAST_OTHER_MIN_BLOCKS
+#define WK_FAST_OTHER_MIN_BLOCKS 16
+#endif
+
 namespace wk {
 
 int set_error(int code, const std::string& msg);

@@ -1440,7 +1440,7 @@ int wake_grid_compute_vorticity(wake_grid* g, float* vorticity) {
         WK_CUDA(g->m_an.ensure(b));
         out = g->m_an.as<float>();
     }
-    k_vorticity_2d<<<analytics_grid_3d(g->nx, g->ny, 1, 128), 128, 0, g->stream>>>(
+    k_vorticity_2d<<<analytics_grid_3d(g->nx, g->ny, 1), analytics_block(), 0, g->stream>>>(
         g->m_ux.as<float>(), g->m_uy.as<float>(), out, g->nx, g->ny);
     WK_CUDA(cudaGetLastError());
     if (out != vorticity) WK_CUDA(cudaMemcpyAsync(vorticity, out, b, cudaMemcpyDeviceToHost, g->stream));
@@ -1463,7 +1463,7 @@ int wake_grid_compute_3d_features(wake_grid* g, float* omega_x, float* omega_y, 
     for (int i = 0; i < 4; ++i) staged = staged || !on_device(user[i]);
     if (staged) WK_CUDA(g->m_an.ensure(4 * b));
     for (int i = 0; i < 4; ++i) out[i] = on_device(user[i]) ? user[i] : g->m_an.as<float>() + i * g->N;
-    k_vorticity_q_3d<<<analytics_grid_3d(g->nx, g->ny, g->nz, 128), 128, 0, g->stream>>>(
+    k_vorticity_q_3d<<<analytics_grid_3d(g->nx, g->ny, g->nz), analytics_block(), 0, g->stream>>>(
         g->m_ux.as<float>(), g->m_uy.as<float>(), g->m_uz.as<float>(), out[0], out[1], out[2], out[3], g->nx, g->ny,
         g->nz);
     WK_CUDA(cudaGetLastError());

@@ -105,7 +105,7 @@ struct wake_grid {
     // reuse a destroyed grid's address for the old one.
     unsigned long long geom_version = 0;
 
-    int tpb = 0, xchunks = 1, rows = 1, tpb_fast = 256;
+    int tpb = 0, xchunks = 1, rows = 1, tpb_fast = 64;
     // step kernels: 0 automatic, 1 direct (k_step_fast for the pure-gather rows beside
     // k_step for the rest), 2 persistent tiles (k_step_tiles: pure-gather tiles staged in
     // shared memory plus the general rows, when the row shape allows it)
@@ -218,10 +218,10 @@ struct wake_grid {
         }
         xchunks = (nx + tpb - 1) / tpb;
         rows = ny * nz;
-        // k_step_fast is limited to 256 threads (four blocks per SM). Least idle lanes over the row,
+        // k_step_fast is limited to WK_FAST_MAX_THREADS threads. Least idle lanes over the row,
         // ties to the smaller block: 64-thread blocks measured fastest on 256-node rows (more
         // independent blocks in flight per SM, shorter tail per row).
-        const int cap = std::min(want > 0 ? want : 256, 256);
+        const int cap = std::min(want > 0 ? want : WK_FAST_MAX_THREADS, WK_FAST_MAX_THREADS);
         int best = -1, best_waste = 1 << 30;
         for (int t = 64; t <= cap; t += 32) {
             const int waste = ((nx + t - 1) / t) * t - nx;

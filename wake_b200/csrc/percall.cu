@@ -832,7 +832,8 @@ void compute_vorticity_2d(const float ux[], const float uy[], float vorticity[],
     s.in(uy, n);
     s.full_out(vorticity, n);
     if (s.begin()) return;
-    k_vorticity_2d<<<analytics_grid_3d(nx, ny, 1, 128), 128>>>(s.ptr<float>(0), s.ptr<float>(1), s.ptr<float>(2), nx, ny);
+    k_vorticity_2d<<<analytics_grid_3d(nx, ny, 1), analytics_block()>>>(s.ptr<float>(0), s.ptr<float>(1),
+                                                                         s.ptr<float>(2), nx, ny);
     s.end();
 }
 
@@ -851,9 +852,9 @@ void compute_vorticity_and_q_criterion_3d(const float ux[], const float uy[], co
     s.full_out(omega_z, n);
     s.full_out(q_criterion, n);
     if (s.begin()) return;
-    k_vorticity_q_3d<<<analytics_grid_3d(nx, ny, nz, 128), 128>>>(s.ptr<float>(0), s.ptr<float>(1), s.ptr<float>(2),
-                                                                  s.ptr<float>(3), s.ptr<float>(4), s.ptr<float>(5),
-                                                                  s.ptr<float>(6), nx, ny, nz);
+    k_vorticity_q_3d<<<analytics_grid_3d(nx, ny, nz), analytics_block()>>>(
+        s.ptr<float>(0), s.ptr<float>(1), s.ptr<float>(2), s.ptr<float>(3), s.ptr<float>(4), s.ptr<float>(5),
+        s.ptr<float>(6), nx, ny, nz);
     s.end();
 }
 

@@ -15,6 +15,7 @@
 // 2*Q*sizeof(pop) + 1 flag byte per node through HBM.
 #pragma once
 
+#include "common.cuh"
 #include "lattice.cuh"
 #include "pairs2.cuh"
 
@@ -449,20 +450,36 @@ __device__ __forceinline__ void step_span_fast2(const StepArgs& a, const Seg& sg
         const bool vb = xa + 32 < sg.x1;
         const int xb = vb ? xa + 32 : xa;  // a short chunk computes node a twice and stores it once
         const uint8_t fa = a.flags[row0 + xa], fb = a.flags[row0 + xb];
-        const int xsa[3] = {xa + 1 == nx ? 0 : xa + 1, xa, xa == 0 ? nx - 1 : xa - 1};
-        const int xsb[3] = {xb + 1 == nx ? 0 : xb + 1, xb, xb == 0 ? nx - 1 : xb - 1};
         float2 f[Q];
+        // A full chunk away from x = 0 and x = nx - 1 (the warp-uniform common case) has
+        // node b = node a + 32 in every plane, with no wrap: both loads of a direction share
+        // one address, and the three x shifts are three per-thread pointers.
+        const bool inner = IDX32 && base >= 1 && base + 64 < nx && base + 64 <= sg.x1;
+        if (inner) {
+            const unsigned P = static_cast<unsigned>(a.geo.pitch);
+            const T* px[3] = {fin + (xa + 1), fin + xa, fin + (xa - 1)};  // source x - c_x for c_x = -1, 0, 1
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            if constexpr (IDX32) {
-                const unsigned P = static_cast<unsigned>(a.geo.pitch);
+            for (int q = 0; q < Q; ++q) {
                 const unsigned rowsrc = static_cast<unsigned>((zsrc[L::cz(q) + 1] * ny + ysrc[L::cy(q) + 1]) * nx);
-                const T* pl = fin + (q * P + rowsrc);
-                f[q] = make_float2(load_raw<S>(pl + xsa[L::cx(q) + 1]), load_raw<S>(pl + xsb[L::cx(q) + 1]));
-            } else {
-                const long long rowsrc = (static_cast<long long>(zsrc[L::cz(q) + 1]) * ny + ysrc[L::cy(q) + 1]) * nx;
-                const T* pl = fin + (q * a.geo.pitch + rowsrc);
-                f[q] = make_float2(load_raw<S>(pl + xsa[L::cx(q) + 1]), load_raw<S>(pl + xsb[L::cx(q) + 1]));
+                const T* pl = px[L::cx(q) + 1] + (q * P + rowsrc);
+                f[q] = make_float2(load_raw<S>(pl), load_raw<S>(pl + 32));
+            }
+        }
+        if (!inner) {
+            const int xsa[3] = {xa + 1 == nx ? 0 : xa + 1, xa, xa == 0 ? nx - 1 : xa - 1};
+            const int xsb[3] = {xb + 1 == nx ? 0 : xb + 1, xb, xb == 0 ? nx - 1 : xb - 1};
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                if constexpr (IDX32) {
+                    const unsigned P = static_cast<unsigned>(a.geo.pitch);
+                    const unsigned rowsrc = static_cast<unsigned>((zsrc[L::cz(q) + 1] * ny + ysrc[L::cy(q) + 1]) * nx);
+                    const T* pl = fin + (q * P + rowsrc);
+                    f[q] = make_float2(load_raw<S>(pl + xsa[L::cx(q) + 1]), load_raw<S>(pl + xsb[L::cx(q) + 1]));
+                } else {
+                    const long long rowsrc = (static_cast<long long>(zsrc[L::cz(q) + 1]) * ny + ysrc[L::cy(q) + 1]) * nx;
+                    const T* pl = fin + (q * a.geo.pitch + rowsrc);
+                    f[q] = make_float2(load_raw<S>(pl + xsa[L::cx(q) + 1]), load_raw<S>(pl + xsb[L::cx(q) + 1]));
+                }
             }
         }
         if ((fa | fb) & (FL_ZH_IN | FL_ZH_OUT)) {
@@ -565,8 +582,11 @@ __global__ void __launch_bounds__(64) k_step(const StepArgs a) {
 }
 
 // TRT segments carry two nodes per thread (twice the registers, half the threads per node).
+// Register budget: WK_FAST_MAX_THREADS / WK_FAST_*_MIN_BLOCKS (common.cuh).
 template <int Q, int COLL, int S, bool LES, bool IDX32>
-__global__ void __launch_bounds__(256, COLL == COLL_TRT ? 2 : 4) k_step_fast(const StepArgs a) {
+__global__ void __launch_bounds__(WK_FAST_MAX_THREADS,
+                                  COLL == COLL_TRT ? WK_FAST_TRT_MIN_BLOCKS : WK_FAST_OTHER_MIN_BLOCKS)
+    k_step_fast(const StepArgs a) {
     step_span_fast<Q, COLL, S, LES, IDX32>(a, span_decode(a.spans[blockIdx.x], a.geo));
 }
 
@@ -611,7 +631,9 @@ __global__ void __launch_bounds__(64) k_step_batch(const BatchArgs b) {
 }
 
 template <int Q, int COLL, int S, bool LES, bool IDX32>
-__global__ void __launch_bounds__(256, COLL == COLL_TRT ? 2 : 4) k_step_fast_batch(const BatchArgs b) {
+__global__ void __launch_bounds__(WK_FAST_MAX_THREADS,
+                                  COLL == COLL_TRT ? WK_FAST_TRT_MIN_BLOCKS : WK_FAST_OTHER_MIN_BLOCKS)
+    k_step_fast_batch(const BatchArgs b) {
     const uint4 sp = b.spans[blockIdx.x];
     const StepArgs a = batch_member(b, sp.x);
     step_span_fast<Q, COLL, S, LES, IDX32>(a, span_decode(sp, a.geo));
