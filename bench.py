@@ -53,17 +53,43 @@ def parse():
     p.add_argument("--no-tgv", action="store_true", help="skip the D3Q27 MRT Taylor-Green 384^3 leg")
     p.add_argument("--tgv-steps", type=int, default=5000, help="steps of the Taylor-Green leg (multiple of 500)")
     p.add_argument("--tgv-only", action="store_true", help="only the Taylor-Green leg (one JSON line)")
+    p.add_argument("--tgv-size", type=int, default=384, help="edge of the Taylor-Green cube (384 = the workload)")
     p.add_argument("--serve-rate", type=float, default=20.0, help="arrival rate of the served-mix leg (jobs/s)")
     p.add_argument("--serve-jobs", type=int, default=60, help="jobs in the served-mix leg")
     p.add_argument("--serve-graph", type=int, default=20, help="steps per CUDA graph inside a served batch (0: plain)")
     p.add_argument("--serve-sweep", default=None,
                    help="comma-separated arrival rates: only the served mix at each rate (one JSON line per rate)")
     p.add_argument("--graph", type=int, default=20, help="steps per captured CUDA graph (0: plain launches)")
-    p.add_argument("--profile", choices=["f32", "f16", "bf16"], default=None,
-                   help="profiling mode: only warm-up + timed steps of this storage, plain launches, one JSON line")
+    p.add_argument("--profile", choices=["f32", "f16", "bf16", "vorticity"], default=None,
+                   help="profiling mode: only warm-up + timed steps of this storage, plain launches, one JSON line "
+                        "('vorticity': --steps calls of the 3D vorticity / Q-criterion kernel on 256^3 device fields)")
     p.add_argument("--block", type=int, default=0, help="threads per block of the fused step (0: automatic)")
     p.add_argument("--kernel", type=int, default=0, help="pure-gather row kernel: 0 auto, 1 direct gather, 2 staged")
     return p.parse_args()
+
+
+def run_vorticity_profile(args, L=256):
+    """Small command for ncu: the 3D vorticity / Q-criterion drop-in on device fields of L^3 nodes
+    (three 67 MB inputs, four 67 MB outputs at L = 256: larger than L2)."""
+    import torch
+
+    import wake_b200 as wb
+    from wake_b200 import workloads as W
+
+    u = W.taylor_green_fields_device(L, 0.04)[1:]
+    out = torch.empty((4, L ** 3), dtype=torch.float32, device="cuda")
+    times = []
+    for i in range(args.warmup + args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(torch.cuda.default_stream())
+        wb.lib.compute_vorticity_and_q_criterion_3d(*[a.data_ptr() for a in u], *[o.data_ptr() for o in out], L, L, L)
+        e1.record(torch.cuda.default_stream())
+        e1.synchronize()
+        if i >= args.warmup:
+            times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times) if times else float("nan")
+    print(json.dumps({"profile": "vorticity", "nodes": L ** 3, "calls": args.steps, "ms_per_call": ms,
+                      "achieved_gbs": 28 * L ** 3 / (ms * 1e-3) / 1e9}))
 
 
 def run_profile(args):
@@ -73,6 +99,10 @@ def run_profile(args):
     from wake_b200 import workloads as W
 
     import wake_b200 as wb
+
+    if args.profile == "vorticity":
+        run_vorticity_profile(args)
+        return
 
     case = W.sphere_channel()
     g = W.build_grid(case, storage=args.profile)
@@ -408,7 +438,7 @@ def tgv_leg(L=384, steps=5000, every=500, graph=20):
             if st != "f32":
                 row[f"u_rel_l2_{st}_vs_f32"] = torch.linalg.vector_norm((u[st] - u["f32"]).double()).item() / ref_norm
         rows.append(row)
-    out = {"workload": TGV_WORKLOAD, "nodes": n, "steps": steps, "timed_steps": timed_steps_done,
+    out = {"workload": TGV_WORKLOAD.replace("384^3", f"{L}^3"), "nodes": n, "steps": steps, "timed_steps": timed_steps_done,
            "graph_steps": graph, "checkpoints": rows}
     peak, _ = hbm_peak()
     for st in grids:
@@ -532,7 +562,7 @@ def main():
                                                                           graph_steps=args.serve_graph)}), flush=True)
         return
     if args.tgv_only:
-        print(json.dumps(tgv_leg(steps=args.tgv_steps)))
+        print(json.dumps(tgv_leg(L=args.tgv_size, steps=args.tgv_steps)))
         return
     if args.batch_only:
         out = {"workload": BATCH_WORKLOAD, "f32": batched_leg("f32"), "f16": batched_leg("f16")}
@@ -626,7 +656,7 @@ def main():
         batched = {"workload": BATCH_WORKLOAD, "f32": batched_leg("f32"), "f16": batched_leg("f16")}
     tgv = None
     if not args.no_tgv:
-        tgv = tgv_leg(steps=args.tgv_steps)
+        tgv = tgv_leg(L=args.tgv_size, steps=args.tgv_steps)
     served = None
     if not args.no_serve:
         served = {"workload": SERVE_WORKLOAD, **serving_leg(args.serve_rate, args.serve_jobs)}

@@ -267,6 +267,29 @@ def percall_cases(R):
     save("percall", **res)
 
 
+def c1_case(R, steps=20000):
+    """The full D2Q9 BGK cylinder channel (400x160, D = 20 at (80, 80), tau = 0.56, seeded 1e-4
+    noise): the reference's own 20,000 steps with momentum exchange (r_max = 1.5 D) every step,
+    as KarmanVortexScenario runs it (src/scenarios/karman_vortex.cpp:62-124). Stores the force
+    history and the reference's Strouhal frequency of its lift (StrouhalAnalyzer, first 4096
+    samples)."""
+    c = W.cylinder_channel()
+    g = oracle.RefGrid2D(c.nx, c.ny, c.tau)
+    g.init_fields(c.rho, c.ux, c.uy)
+    R.ref2d_set_inflow_west(g._h, 0.05, 0.0)
+    R.ref2d_set_outflow_east(g._h, 1.0)
+    for x in range(c.nx):
+        R.ref2d_set_cell_type(g._h, x, 0, 1)
+        R.ref2d_set_cell_type(g._h, x, c.ny - 1, 1)
+    R.ref2d_set_solid_circle(g._h, 80.0, 80.0, 10.0)
+    assert (g.cell_types() == c.types).all()
+    hist = g.step_forces(steps, 0, 80.0, 80.0, 30.0)
+    cl = (hist[:, 1] / (0.5 * 0.05 ** 2 * 20.0)).astype(np.float32)
+    f_ref = R.ref_strouhal_frequency(a(cl), len(cl), 1.0)
+    save("c1_cyl2d_bgk", forces=hist.astype(np.float32), steps=np.int32(steps), tau=np.float32(c.tau),
+         strouhal_freq=np.float32(f_ref))
+
+
 def kat_cases(R):
     # Strouhal FFT KAT (tests/unit/test_forces_momentum_exchange.cpp:71-91)
     t = np.arange(512, dtype=np.float32)
@@ -287,7 +310,11 @@ def main():
     tgv_case(R)
     percall_cases(R)
     kat_cases(R)
+    c1_case(R)
 
 
 if __name__ == "__main__":
-    main()
+    if "--c1" in sys.argv:  # only the long C1 run
+        c1_case(oracle.ref())
+    else:
+        main()

@@ -451,35 +451,19 @@ __device__ __forceinline__ void step_span_fast2(const StepArgs& a, const Seg& sg
         const int xb = vb ? xa + 32 : xa;  // a short chunk computes node a twice and stores it once
         const uint8_t fa = a.flags[row0 + xa], fb = a.flags[row0 + xb];
         float2 f[Q];
-        // A full chunk away from x = 0 and x = nx - 1 (the warp-uniform common case) has
-        // node b = node a + 32 in every plane, with no wrap: both loads of a direction share
-        // one address, and the three x shifts are three per-thread pointers.
-        const bool inner = IDX32 && base >= 1 && base + 64 < nx && base + 64 <= sg.x1;
-        if (inner) {
-            const unsigned P = static_cast<unsigned>(a.geo.pitch);
-            const T* px[3] = {fin + (xa + 1), fin + xa, fin + (xa - 1)};  // source x - c_x for c_x = -1, 0, 1
+        const int xsa[3] = {xa + 1 == nx ? 0 : xa + 1, xa, xa == 0 ? nx - 1 : xa - 1};
+        const int xsb[3] = {xb + 1 == nx ? 0 : xb + 1, xb, xb == 0 ? nx - 1 : xb - 1};
 #pragma unroll
-            for (int q = 0; q < Q; ++q) {
+        for (int q = 0; q < Q; ++q) {
+            if constexpr (IDX32) {
+                const unsigned P = static_cast<unsigned>(a.geo.pitch);
                 const unsigned rowsrc = static_cast<unsigned>((zsrc[L::cz(q) + 1] * ny + ysrc[L::cy(q) + 1]) * nx);
-                const T* pl = px[L::cx(q) + 1] + (q * P + rowsrc);
-                f[q] = make_float2(load_raw<S>(pl), load_raw<S>(pl + 32));
-            }
-        }
-        if (!inner) {
-            const int xsa[3] = {xa + 1 == nx ? 0 : xa + 1, xa, xa == 0 ? nx - 1 : xa - 1};
-            const int xsb[3] = {xb + 1 == nx ? 0 : xb + 1, xb, xb == 0 ? nx - 1 : xb - 1};
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                if constexpr (IDX32) {
-                    const unsigned P = static_cast<unsigned>(a.geo.pitch);
-                    const unsigned rowsrc = static_cast<unsigned>((zsrc[L::cz(q) + 1] * ny + ysrc[L::cy(q) + 1]) * nx);
-                    const T* pl = fin + (q * P + rowsrc);
-                    f[q] = make_float2(load_raw<S>(pl + xsa[L::cx(q) + 1]), load_raw<S>(pl + xsb[L::cx(q) + 1]));
-                } else {
-                    const long long rowsrc = (static_cast<long long>(zsrc[L::cz(q) + 1]) * ny + ysrc[L::cy(q) + 1]) * nx;
-                    const T* pl = fin + (q * a.geo.pitch + rowsrc);
-                    f[q] = make_float2(load_raw<S>(pl + xsa[L::cx(q) + 1]), load_raw<S>(pl + xsb[L::cx(q) + 1]));
-                }
+                const T* pl = fin + (q * P + rowsrc);
+                f[q] = make_float2(load_raw<S>(pl + xsa[L::cx(q) + 1]), load_raw<S>(pl + xsb[L::cx(q) + 1]));
+            } else {
+                const long long rowsrc = (static_cast<long long>(zsrc[L::cz(q) + 1]) * ny + ysrc[L::cy(q) + 1]) * nx;
+                const T* pl = fin + (q * a.geo.pitch + rowsrc);
+                f[q] = make_float2(load_raw<S>(pl + xsa[L::cx(q) + 1]), load_raw<S>(pl + xsb[L::cx(q) + 1]));
             }
         }
         if ((fa | fb) & (FL_ZH_IN | FL_ZH_OUT)) {
