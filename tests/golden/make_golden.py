@@ -283,11 +283,21 @@ def c1_case(R, steps=20000):
         R.ref2d_set_cell_type(g._h, x, c.ny - 1, 1)
     R.ref2d_set_solid_circle(g._h, 80.0, 80.0, 10.0)
     assert (g.cell_types() == c.types).all()
+    f0 = g.f()
     hist = g.step_forces(steps, 0, 80.0, 80.0, 30.0)
     cl = (hist[:, 1] / (0.5 * 0.05 ** 2 * 20.0)).astype(np.float32)
     f_ref = R.ref_strouhal_frequency(a(cl), len(cl), 1.0)
-    save("c1_cyl2d_bgk", forces=hist.astype(np.float32), steps=np.int32(steps), tau=np.float32(c.tau),
-         strouhal_freq=np.float32(f_ref))
+    # the same run in the FP64 oracle, the yardstick for the FP32 drift of either implementation
+    o = oracle.OracleGrid(9, c.nx, c.ny, 1, 64)
+    o.configure(collision=0, tau=c.tau, inflow=1, outflow=1, u_in=(0.05, 0.0, 0.0), rho_out=1.0, mem=1,
+                center=(80.0, 80.0, 0.0), r_max=30.0)
+    o.set_cell_types(c.types)
+    o.set_state(f0)
+    h64 = o.step(steps, forces=True)
+    # Fx, Fy per step; the FP64 history rounded to float32 (6e-8 relative, far below its 5e-5 gap to FP32)
+    save("c1_cyl2d_bgk", forces=hist[:, :2].astype(np.float32), forces_fp64=h64[:, :2].astype(np.float32),
+         steps=np.int32(steps),
+         tau=np.float32(c.tau), strouhal_freq=np.float32(f_ref), f0_sum=np.float64(f0.astype(np.float64).sum()))
 
 
 def kat_cases(R):

@@ -342,3 +342,43 @@ def test_staged_and_direct_kernels_agree(storage, which):
     assert np.array_equal(out[0][0], out[1][0])
     if case.mem:
         assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_c1_cylinder_channel_full_length_tracks_reference(golden):
+    """C1 at full length: D2Q9 BGK cylinder channel 400x160 (D = 20), 20,000 steps from the
+    seeded initial state, momentum exchange (r_max = 1.5 D) every step, as the reference's
+    KarmanVortexScenario runs it. Fixture: the reference's own force history and, for the same
+    run, the FP64 oracle's (tests/golden/make_golden.py). The drag history stays within 1e-4
+    (relative L2) of the reference; drag and lift stay as close to FP64 as the reference does;
+    and the Strouhal analysis of the lift (mean removed, Hann window, first 4096 samples, as
+    the reference analyses it) finds the reference's frequency."""
+    d = golden("c1_cyl2d_bgk")
+    steps = int(d["steps"])
+    c = W.cylinder_channel()
+    g = W.build_grid(c)
+    # same initial populations as the reference run (seeded noise, reference float order)
+    f0_sum = g.f_src_data().astype(np.float64).sum()
+    assert abs(f0_sum - float(d["f0_sum"])) <= 1e-12 * float(d["f0_sum"]), f0_sum - float(d["f0_sum"])
+    g.use_graph(20)
+    g.step(c.collision, n=steps)
+    g.synchronize()
+    hist = g.force_history()
+    g.close()
+    assert hist.shape == (steps, 3)
+    q = 0.5 * 0.05 ** 2 * 20.0
+    ours = hist[:, :2] / q
+    ref = d["forces"].astype(np.float64) / q
+    r64 = d["forces_fp64"].astype(np.float64) / q
+    e = {k: (rel_l2(ours[:, i], ref[:, i]), rel_l2(ours[:, i], r64[:, i]), rel_l2(ref[:, i], r64[:, i]))
+         for i, k in enumerate(("CD", "CL"))}
+    tail_cd = abs(ours[-5000:, 0].mean() - ref[-5000:, 0].mean()) / abs(ref[-5000:, 0].mean())
+    f_ours = wb.strouhal_frequency(ours[:4096, 1], 1.0)
+    f_ref = float(d["strouhal_freq"])
+    print(f"[C1 20k] CD gpu-ref {e['CD'][0]:.2e} gpu-fp64 {e['CD'][1]:.2e} ref-fp64 {e['CD'][2]:.2e} | "
+          f"CL gpu-ref {e['CL'][0]:.2e} gpu-fp64 {e['CL'][1]:.2e} ref-fp64 {e['CL'][2]:.2e} | "
+          f"mean CD (last 5000) {tail_cd:.2e} | f {f_ours:.6f} vs ref {f_ref:.6f} (St {f_ours * 20 / 0.05:.3f})")
+    assert e["CD"][0] <= FORCE_TOL
+    assert tail_cd <= FORCE_TOL
+    for k in ("CD", "CL"):
+        assert e[k][1] <= 2.0 * e[k][2] + 1e-5, k
+    assert abs(f_ours - f_ref) <= 1.0 / 4096 + 1e-7
