@@ -300,6 +300,48 @@ def c1_case(R, steps=20000):
          tau=np.float32(c.tau), strouhal_freq=np.float32(f_ref), f0_sum=np.float64(f0.astype(np.float64).sum()))
 
 
+def c2_case(R, steps=2000):
+    """The D3Q19 sphere channel at full size (256x128x128, sphere R = 12 at (64, 64, 64), TRT with
+    Lambda = 1/4, tau0 = 0.52, 2000 steps) in the form the reference can run: x-periodic, y/z
+    half-way walls, no Zou-He, LES computed but not applied. The reference's own run gives the
+    per-step force history and the moments on two planes through the sphere (z = 64 and y = 64);
+    the FP64 oracle runs the same case from the same populations and links, and its results are
+    stored rounded to float32 (6e-8 relative, far below their 1e-5 gap to FP32)."""
+    c = W.sphere_channel(reference_variant=True, collision=1, les=False)
+    cx, cy, cz, r = c.sphere
+    g = oracle.RefGrid3D(c.nx, c.ny, c.nz, c.tau)
+    g.init_fields(c.rho, c.ux, c.uy, c.uz)
+    R.ref3d_set_periodic(g._h, 1)
+    R.ref3d_set_solid_sphere(g._h, cx, cy, cz, r)
+    R.ref3d_build_curved_sphere_links(g._h, cx, cy, cz, r)
+    assert (g.cell_types() == c.types).all()
+    idx, q, d = g.links()
+    f0 = g.f()
+    hist = g.step_forces(steps, 1, (cx, cy, cz), c.mem[3])
+    m = g.macro()
+
+    def planes(fields):
+        out = {}
+        for k in ("rho", "ux", "uy", "uz"):
+            a = np.asarray(fields[k]).reshape(c.nz, c.ny, c.nx)
+            out[f"{k}_z64"] = a[64].astype(np.float32)
+            out[f"{k}_y64"] = a[:, 64, :].astype(np.float32)
+        return out
+
+    o = oracle.OracleGrid(19, c.nx, c.ny, c.nz, 64)
+    o.configure(collision=1, tau=c.tau, les=0, periodic_y=0, periodic_z=0, mem=1, center=(cx, cy, cz),
+                r_max=c.mem[3])
+    o.set_cell_types(c.types)
+    o.set_state(f0)
+    o.set_links(idx, q, d)
+    h64 = o.step(steps, forces=True)
+    m64 = o.macro()
+    ref_planes, o_planes = planes(m), planes(m64)
+    save("c2_sphere3d_trt", steps=np.int32(steps), tau=np.float32(c.tau), forces=hist.astype(np.float32),
+         forces_fp64=h64.astype(np.float32), n_links=np.int32(len(idx)),
+         **{f"ref_{k}": v for k, v in ref_planes.items()}, **{f"fp64_{k}": v for k, v in o_planes.items()})
+
+
 def kat_cases(R):
     # Strouhal FFT KAT (tests/unit/test_forces_momentum_exchange.cpp:71-91)
     t = np.arange(512, dtype=np.float32)
@@ -321,10 +363,13 @@ def main():
     percall_cases(R)
     kat_cases(R)
     c1_case(R)
+    c2_case(R)
 
 
 if __name__ == "__main__":
     if "--c1" in sys.argv:  # only the long C1 run
         c1_case(oracle.ref())
+    elif "--c2" in sys.argv:  # only the full-size C2 run (about an hour on one core)
+        c2_case(oracle.ref())
     else:
         main()

@@ -7,6 +7,8 @@ Tolerances (FP32 arithmetic on both sides, different summation orders):
 Every case also reports its error against the FP64 oracle next to the
 reference's own error against it.
 """
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -382,3 +384,50 @@ def test_c1_cylinder_channel_full_length_tracks_reference(golden):
     for k in ("CD", "CL"):
         assert e[k][1] <= 2.0 * e[k][2] + 1e-5, k
     assert abs(f_ours - f_ref) <= 1.0 / 4096 + 1e-7
+
+
+C2_FIXTURE = Path(__file__).resolve().parent / "golden" / "c2_sphere3d_trt.npz"
+
+
+@pytest.mark.skipif(not C2_FIXTURE.exists(), reason="full-size C2 fixture not generated")
+def test_c2_sphere_channel_full_size_tracks_reference(golden):
+    """C2 at full size and length in the form the reference can run: D3Q19 TRT (Lambda = 1/4),
+    tau0 = 0.52, 256x128x128, sphere R = 12 with BFL links, x-periodic, y/z walls, 2000 steps.
+    Fixture: the reference's own run (force history; rho and u on the planes z = 64 and y = 64
+    through the sphere) and the FP64 oracle's run of the same case. The GPU drag history stays
+    within 1e-4 (relative L2) of the reference's; rho and u on both planes within 1e-5 of it, or
+    within the reference's own distance to FP64 where that is larger; and the GPU is as close to
+    FP64 as the reference."""
+    d = golden("c2_sphere3d_trt")
+    steps = int(d["steps"])
+    c = W.sphere_channel(reference_variant=True, collision=1, les=False)
+    g = W.build_grid(c)
+    assert wb.lib.wake_grid_num_curved_links(g.handle) == int(d["n_links"])
+    g.use_graph(20)
+    g.step(c.collision, use_les=False, n=steps)
+    g.synchronize()
+    m = g.macro()
+    hist = g.force_history()
+    g.close()
+    area = np.pi * 12.0 ** 2
+    q = 0.5 * 0.05 ** 2 * area
+    ours = hist[:, :2] / q
+    ref = d["forces"][:, :2].astype(np.float64) / q
+    r64 = d["forces_fp64"][:, :2].astype(np.float64) / q
+    e_cd = (rel_l2(ours[:, 0], ref[:, 0]), rel_l2(ours[:, 0], r64[:, 0]), rel_l2(ref[:, 0], r64[:, 0]))
+    planes = {}
+    for k in ("rho", "ux", "uy", "uz"):
+        a = m[k].reshape(c.nz, c.ny, c.nx)
+        planes[k] = np.concatenate([a[64].ravel(), a[:, 64, :].ravel()])
+    refp = {k: np.concatenate([d[f"ref_{k}_z64"].ravel(), d[f"ref_{k}_y64"].ravel()]) for k in planes}
+    p64 = {k: np.concatenate([d[f"fp64_{k}_z64"].ravel(), d[f"fp64_{k}_y64"].ravel()]) for k in planes}
+    comps = ("ux", "uy", "uz")
+    e_u = (vel_rel_l2(planes, refp, comps), vel_rel_l2(planes, p64, comps), vel_rel_l2(refp, p64, comps))
+    e_rho = (rel_l2(planes["rho"], refp["rho"]), rel_l2(planes["rho"], p64["rho"]), rel_l2(refp["rho"], p64["rho"]))
+    print(f"[C2 2000 steps] CD gpu-ref {e_cd[0]:.2e} gpu-fp64 {e_cd[1]:.2e} ref-fp64 {e_cd[2]:.2e} | "
+          f"u gpu-ref {e_u[0]:.2e} gpu-fp64 {e_u[1]:.2e} ref-fp64 {e_u[2]:.2e} | "
+          f"rho gpu-ref {e_rho[0]:.2e} gpu-fp64 {e_rho[1]:.2e} ref-fp64 {e_rho[2]:.2e}")
+    assert e_cd[0] <= FORCE_TOL
+    assert e_u[0] <= max(U_TOL, 2.0 * e_u[2]) and e_rho[0] <= max(RHO_TOL, 2.0 * e_rho[2])
+    for e in (e_cd, e_u, e_rho):
+        assert e[1] <= 2.0 * e[2] + 1e-6

@@ -403,6 +403,31 @@ __device__ __forceinline__ void store_raw(typename Codec<S>::T* p, float v) {
     else __stcs(reinterpret_cast<unsigned short*>(p), __bfloat16_as_ushort(__float2bfloat16_rn(v)));
 }
 
+// The two 16-bit values of a 32-bit word (little endian: node x in the low half) as floats,
+// and two floats stored as one rounded 16-bit pair (streaming store).
+template <int S>
+__device__ __forceinline__ float raw_lo(unsigned w) {
+    if constexpr (S == STORE_F16) return __half2float(__ushort_as_half(static_cast<unsigned short>(w & 0xffffu)));
+    else return __bfloat162float(__ushort_as_bfloat16(static_cast<unsigned short>(w & 0xffffu)));
+}
+template <int S>
+__device__ __forceinline__ float raw_hi(unsigned w) {
+    if constexpr (S == STORE_F16) return __half2float(__ushort_as_half(static_cast<unsigned short>(w >> 16)));
+    else return __bfloat162float(__ushort_as_bfloat16(static_cast<unsigned short>(w >> 16)));
+}
+template <int S>
+__device__ __forceinline__ void store_pair(typename Codec<S>::T* p, float2 v) {
+    unsigned w;
+    if constexpr (S == STORE_F16) {
+        const __half2 h = __floats2half2_rn(v.x, v.y);  // .x in the low half
+        w = *reinterpret_cast<const unsigned*>(&h);
+    } else {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
+        w = *reinterpret_cast<const unsigned*>(&h);
+    }
+    __stcs(reinterpret_cast<unsigned*>(p), w);
+}
+
 // Zou-He on one of the two nodes of a packed pair (lane 0 = .x, 1 = .y); the
 // formulas work on f, so shifted values are decoded and encoded around them.
 template <int Q, bool HS>
@@ -424,6 +449,71 @@ __device__ __forceinline__ void zou_he_half(float2* f, int lane, uint8_t fl, con
     }
 }
 
+// 16-bit storage with adjacent node pairs: a thread steps nodes x and x + 1 (x even),
+// which sit in one 32-bit word of every plane. Directions without an x component
+// load both nodes with one 32-bit load; every direction stores both with one packed
+// conversion and one 32-bit store. Needs nx even (every row, hence every pair, starts
+// on a 4-byte boundary; the plane pitch is a multiple of 64) and an even span start.
+// The arithmetic is the same per node as in step_span_fast2, so results are identical.
+template <int Q, int S, bool LES>
+__device__ __forceinline__ void step_span_adjacent(const StepArgs& a, const Seg& sg) {
+    using L = Lat<Q>;
+    using C = Codec<S>;
+    using T = typename C::T;
+    const int nx = a.geo.nx, ny = a.geo.ny, nz = a.geo.nz;
+    const int y = sg.y, z = sg.z;
+    const unsigned row0 = static_cast<unsigned>(sg.row0);
+    const int yl = (y + 1 == ny) ? (a.geo.periodic_y ? 0 : y + 1) : y + 1;
+    const int yh = (y == 0) ? (a.geo.periodic_y ? ny - 1 : -1) : y - 1;
+    const int zl = (z + 1 == nz) ? (a.geo.periodic_z ? 0 : z + 1) : z + 1;
+    const int zh = (z == 0) ? (a.geo.periodic_z ? nz - 1 : -1) : z - 1;
+    const int ysrc[3] = {yl, y, yh}, zsrc[3] = {zl, z, zh};
+    const T* fin = static_cast<const T*>(a.fin);
+    T* out = static_cast<T*>(a.fout);
+    const unsigned P = static_cast<unsigned>(a.geo.pitch);
+    const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (int base = sg.x0 + (threadIdx.x >> 5) * 64; base < sg.x1; base += nwarps * 64) {
+        const int xa = base + 2 * lane;  // even
+        if (xa >= sg.x1) continue;
+        const bool vb = xa + 1 < sg.x1;  // node b = xa + 1 < nx always (nx even); unused when outside the span
+        const uint8_t fa = a.flags[row0 + xa], fb = vb ? a.flags[row0 + xa + 1] : fa;
+        float2 f[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const unsigned rowsrc = static_cast<unsigned>((zsrc[L::cz(q) + 1] * ny + ysrc[L::cy(q) + 1]) * nx);
+            const T* pl = fin + (q * P + rowsrc);
+            if (L::cx(q) == 0) {
+                const unsigned w = __ldg(reinterpret_cast<const unsigned*>(pl + xa));
+                f[q] = make_float2(raw_lo<S>(w), raw_hi<S>(w));
+            } else {
+                // source x - c_x of each node, wrapped in x
+                int sa = xa - L::cx(q), sb = xa + 1 - L::cx(q);
+                sa = sa < 0 ? sa + nx : (sa >= nx ? sa - nx : sa);
+                sb = sb < 0 ? sb + nx : (sb >= nx ? sb - nx : sb);
+                f[q] = make_float2(load_raw<S>(pl + sa), load_raw<S>(pl + sb));
+            }
+        }
+        if (!vb) {  // node b lies outside the span: step a copy of node a, store nothing
+#pragma unroll
+            for (int q = 0; q < Q; ++q) f[q].y = f[q].x;
+        }
+        if ((fa | fb) & (FL_ZH_IN | FL_ZH_OUT)) {
+            if (fa & (FL_ZH_IN | FL_ZH_OUT)) zou_he_half<Q, true>(f, 0, fa, a.geo);
+            if (vb && (fb & (FL_ZH_IN | FL_ZH_OUT))) zou_he_half<Q, true>(f, 1, fb, a.geo);
+        }
+        float2 rho, u[3];
+        trt_pairs2<Q, LES, true>(f, a.phys, rho, u);
+        const bool bad = !(rho.x > 0.0f) || !(fabsf(u[0].x) < 1e30f) || (vb && (!(rho.y > 0.0f) || !(fabsf(u[0].y) < 1e30f)));
+        if (bad) atomicOr(a.status, ERR_NONFINITE);
+        T* oa = out + (row0 + xa);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            if (vb) store_pair<S>(oa + q * P, f[q]);
+            else store_raw<S>(oa + q * P, f[q].x);
+        }
+    }
+}
+
 // TRT pure-gather span, one block: each warp takes 64-node chunks, two nodes per
 // thread (base + lane and base + lane + 32) in packed FP32 (trt_pairs2); shifted
 // storage is updated in h directly.
@@ -433,6 +523,12 @@ __device__ __forceinline__ void step_span_fast2(const StepArgs& a, const Seg& sg
     using C = Codec<S>;
     using T = typename C::T;
     constexpr bool HS = S != STORE_F32;
+    if constexpr (HS && IDX32) {
+        if ((a.geo.nx & 1) == 0 && (sg.x0 & 1) == 0) {  // uniform over the block
+            step_span_adjacent<Q, S, LES>(a, sg);
+            return;
+        }
+    }
     const int nx = a.geo.nx, ny = a.geo.ny, nz = a.geo.nz;
     const int y = sg.y, z = sg.z;
     const long long row0 = sg.row0;
