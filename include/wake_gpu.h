@@ -363,6 +363,10 @@ int wake_batch_info(wake_batch* b, long long* nodes, int* bulk_rows, int* genera
  * the build's bound, 64 by default) and keeps the fastest; members advance
  * `steps` per size tried. Results do not depend on the choice. */
 int wake_batch_autotune(wake_batch* b, int steps, int* best_threads);
+/* Host seconds spent so far inside wake_batch_step, by phase: preparing members and
+ * tables, capturing and instantiating CUDA graphs, issuing launches (including any wait
+ * for launch-queue space). For finding where a serving loop's time goes. */
+int wake_batch_host_seconds(wake_batch* b, double* prepare_s, double* capture_s, double* launch_s);
 
 /* ------------------------------------------------------------------ field analytics and VTK
  * FieldAnalytics (src/analytics/field_analytics.cpp:18-63) on the device, from

@@ -136,6 +136,7 @@ _PROTOS = {
     "wake_batch_synchronize": (I, [vp]),
     "wake_batch_info": (I, [vp, vp, vp, vp, vp]),
     "wake_batch_autotune": (I, [vp, I, vp]),
+    "wake_batch_host_seconds": (I, [vp, vp, vp, vp]),
     "wake_grid_compute_vorticity": (I, [vp, vp]),
     "wake_grid_compute_3d_features": (I, [vp, vp, vp, vp, vp]),
     "wake_grid_max_vorticity": (I, [vp, vp]),

@@ -94,6 +94,12 @@ class Batch:
         check(lib.wake_batch_autotune(self._h, steps, ctypes.byref(best)))
         return best.value
 
+    def host_seconds(self) -> dict:
+        """Host time spent inside step() so far: member/table preparation, graph capture, launches."""
+        v = [ctypes.c_double() for _ in range(3)]
+        check(lib.wake_batch_host_seconds(self._h, *[ctypes.byref(x) for x in v]))
+        return {"prepare": v[0].value, "capture": v[1].value, "launch": v[2].value}
+
     def synchronize(self) -> None:
         check(lib.wake_batch_synchronize(self._h))
 

@@ -12,6 +12,7 @@
 // Each launch reads the member's step arguments from a device table, so members
 // of any size share a launch and the per-node arithmetic is the single-lattice
 // arithmetic: a member's results do not depend on what else is in the batch.
+#include <chrono>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -64,6 +65,9 @@ struct wake_batch {
     std::vector<std::pair<const wake_grid*, unsigned long long>> layout;
     std::vector<int> gen_first;
     unsigned shape = 0;  // bumped when launch shapes or table addresses change
+    // host seconds spent in wake_batch_step: preparing members and tables, capturing and
+    // instantiating graphs, issuing launches (a launch that waits for queue space counts here)
+    double host_s[3] = {0.0, 0.0, 0.0};
 
     int tpb_fast = 64, tpb_gen = 128;
 
@@ -389,7 +393,15 @@ int wake_batch_step(wake_batch* b, int n) {
     if (!valid_batch(b)) return WAKE_ERR_INVALID;
     if (n < 0) return set_error(WAKE_ERR_INVALID, "negative step count");
     if (n == 0 || b->members.empty()) return WAKE_OK;
+    using clock = std::chrono::steady_clock;
+    auto t0 = clock::now();
+    auto lap = [&](int phase) {
+        const auto t = clock::now();
+        b->host_s[phase] += std::chrono::duration<double>(t - t0).count();
+        t0 = t;
+    };
     int r = batch_prepare(b);
+    lap(0);
     if (r) return r;
     int done = 0;
     const int gs = b->graph_steps;
@@ -416,6 +428,7 @@ int wake_batch_step(wake_batch* b, int n) {
             b->graph_shape = b->shape;
             b->graph_parity = p0;
         }
+        lap(1);
         while (n - done >= gs) {  // gs is even: the parity returns to graph_parity
             WK_CUDA(cudaGraphLaunch(b->graph, b->stream));
             done += gs;
@@ -423,7 +436,16 @@ int wake_batch_step(wake_batch* b, int n) {
     }
     r = batch_steps(b, n - done);
     for (auto& m : b->members) grid_advanced(m.g, n);
+    lap(2);
     return r;
+}
+
+int wake_batch_host_seconds(wake_batch* b, double* prepare_s, double* capture_s, double* launch_s) {
+    if (!valid_batch(b)) return WAKE_ERR_INVALID;
+    if (prepare_s) *prepare_s = b->host_s[0];
+    if (capture_s) *capture_s = b->host_s[1];
+    if (launch_s) *launch_s = b->host_s[2];
+    return WAKE_OK;
 }
 
 int wake_batch_synchronize(wake_batch* b) {

@@ -280,11 +280,15 @@ class Server:
                 if not staged:
                     time.sleep(max(0.0, min(0.005, pending[0].arrival - now())))
         makespan = now()
+        inside = {"prepare": 0.0, "capture": 0.0, "launch": 0.0}
         for b, _ in batches.values():
+            for k, v in b.host_seconds().items():
+                inside[k] += v
             b.close()
         results.sort(key=lambda r: r.id)
         return ServeReport(results, makespan, ticks, peak, self.budget,
-                           {"host_seconds": {k: round(v, 4) for k, v in phase.items()}})
+                           {"host_seconds": {k: round(v, 4) for k, v in phase.items()},
+                            "batch_step_host_seconds": {k: round(v, 4) for k, v in inside.items()}})
 
 
 def run_alone(job: Job, storage: str = "f32", graph_steps: int = 0) -> JobResult:
