@@ -56,7 +56,7 @@ def parse():
     p.add_argument("--tgv-size", type=int, default=384, help="edge of the Taylor-Green cube (384 = the workload)")
     p.add_argument("--serve-rate", type=float, default=20.0, help="arrival rate of the served-mix leg (jobs/s)")
     p.add_argument("--serve-jobs", type=int, default=60, help="jobs in the served-mix leg")
-    p.add_argument("--serve-graph", type=int, default=20, help="steps per CUDA graph inside a served batch (0: plain)")
+    p.add_argument("--serve-graph", type=int, default=0, help="steps per CUDA graph inside a served batch (0: plain)")
     p.add_argument("--serve-sweep", default=None,
                    help="comma-separated arrival rates: only the served mix at each rate (one JSON line per rate)")
     p.add_argument("--graph", type=int, default=20, help="steps per captured CUDA graph (0: plain launches)")
@@ -357,7 +357,7 @@ SERVE_WORKLOAD = ("served mix: Poisson arrivals of D2Q9 channel jobs (ellipse sw
                   "200-20000), admission by an HBM budget of 80% of free device memory")
 
 
-def serving_leg(rate, n_jobs, storage="f32", baseline=True, graph_steps=20):
+def serving_leg(rate, n_jobs, storage="f32", baseline=True, graph_steps=0):
     """Continuous batching (wake_b200.serve.Server) against one-job-at-a-time plain launches on the same
     arrival list, both in real time. sims/s = jobs / makespan; latency = completion - arrival."""
     import torch
@@ -659,7 +659,8 @@ def main():
         tgv = tgv_leg(L=args.tgv_size, steps=args.tgv_steps)
     served = None
     if not args.no_serve:
-        served = {"workload": SERVE_WORKLOAD, **serving_leg(args.serve_rate, args.serve_jobs)}
+        served = {"workload": SERVE_WORKLOAD, **serving_leg(args.serve_rate, args.serve_jobs,
+                                                            graph_steps=args.serve_graph)}
     clocks.stop()
 
     # ---- CPU baseline (rank 0, N = 1)

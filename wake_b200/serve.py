@@ -178,10 +178,15 @@ def _finish(job: Job, g, arrival, admitted, now, error=None) -> JobResult:
 
 # ------------------------------------------------------------------ server
 class Server:
-    """Admission by HBM budget and slots, continuous batching per job kind."""
+    """Admission by HBM budget and slots, continuous batching per job kind.
+
+    Batches step with plain launches by default (graph_steps = 0). Membership changes at
+    most ticks, and each change would re-capture a graph: on the mixed workload that
+    capture was most of the loop's host time and made no tick shorter, because the device
+    is the bottleneck there."""
 
     def __init__(self, budget_bytes: int, storage: str = "f32", max_tick_steps: int = 100, max_slots: int = 4096,
-                 graph_steps: int = 20):
+                 graph_steps: int = 0):
         self.budget = int(budget_bytes)
         self.storage = storage
         self.max_tick = max_tick_steps
