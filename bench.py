@@ -10,8 +10,10 @@ workload. Seeded synthetic inputs (no dataset).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl wake|reference]
 
-N > 1 runs under torchrun: each rank advances its own replica (no data-path
-collective); timing is the max over ranks of the CUDA-event time.
+N > 1 runs under torchrun: each rank advances its own replica of the sphere
+channel and of the Taylor-Green cube, and takes its share (job id mod N) of the
+batched sweep and of the served jobs. There is no data-path collective; timing is
+the max over ranks of the CUDA-event time.
 """
 from __future__ import annotations
 
@@ -203,27 +205,29 @@ def dist_setup(args):
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+        # NCCL between GPUs; gloo where no GPU is visible (host-side runs of the same logic)
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
 def barrier(world):
     if world > 1:
-        import torch.distributed as dist
+        from wake_b200.shard import Ranks
 
-        dist.barrier()
+        Ranks().barrier()
 
 
 def allmax(world, v):
     if world == 1:
         return v
-    import torch
-    import torch.distributed as dist
+    from wake_b200.shard import Ranks
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return Ranks().max(v)
 
 
 def timed_steps(g, case, steps, warmup, world):
@@ -285,8 +289,12 @@ def batched_leg(storage, n_domains=512, steps=STEPS_PER_SIM, warmup=20, baseline
     from wake_b200 import workloads as W
     from wake_b200.batch import Batch
 
-    cases = W.ellipse_sweep(n_domains)
-    nodes = sum(c.n for c in cases)
+    from wake_b200.shard import Ranks, shard
+
+    ranks = Ranks()
+    all_cases = W.ellipse_sweep(n_domains)
+    nodes = sum(c.n for c in all_cases)
+    cases = shard(all_cases, ranks.rank, ranks.world)  # N GPUs: each batches its share of the sweep
     stream = torch.cuda.Stream()
     b = Batch(9, storage)
     b.set_stream(stream.cuda_stream)
@@ -303,12 +311,13 @@ def batched_leg(storage, n_domains=512, steps=STEPS_PER_SIM, warmup=20, baseline
     b.use_graph(20)
     b.step(warmup)
     torch.cuda.synchronize()
+    ranks.barrier()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0.record(stream)
     b.step(steps)
     t1.record(stream)
     t1.synchronize()
-    ms = t0.elapsed_time(t1)
+    ms = ranks.max(t0.elapsed_time(t1))
     info = b.info()
     unstable = 0
     for g in grids:
@@ -316,6 +325,7 @@ def batched_leg(storage, n_domains=512, steps=STEPS_PER_SIM, warmup=20, baseline
             g.synchronize()
         except wb.WakeError:
             unstable += 1
+    unstable = int(ranks.sum(unstable))
     b.close()
     for g in grids:
         g.close()
@@ -323,10 +333,11 @@ def batched_leg(storage, n_domains=512, steps=STEPS_PER_SIM, warmup=20, baseline
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
 
-    # per-job plain launches on the same jobs' first `baseline_jobs` domains
+    # per-job plain launches on the same jobs' first `baseline_jobs` domains (shared out over the ranks)
     per_job_ms = 0.0
     base_nodes = 0
-    for c in cases[:baseline_jobs]:
+    ranks.barrier()
+    for c in shard(all_cases[:baseline_jobs], ranks.rank, ranks.world):
         g = W.build_grid(c, storage=storage)
         g.set_stream(stream.cuda_stream)
         g.step(c.collision, use_les=c.les, smag_const=c.cs_smag, n=warmup)
@@ -339,6 +350,8 @@ def batched_leg(storage, n_domains=512, steps=STEPS_PER_SIM, warmup=20, baseline
         per_job_ms += e0.elapsed_time(e1)
         base_nodes += c.n
         g.close()
+    per_job_ms = ranks.max(per_job_ms)
+    base_nodes = int(ranks.sum(base_nodes))
     bpn = 2 * 9 * (4 if storage == "f32" else 2) + 1
     sims = n_domains * steps / STEPS_PER_SIM / (ms * 1e-3)
     base_sims = baseline_jobs * steps / STEPS_PER_SIM / (per_job_ms * 1e-3)
@@ -346,7 +359,7 @@ def batched_leg(storage, n_domains=512, steps=STEPS_PER_SIM, warmup=20, baseline
             "nodes": nodes, "steps": steps, "ms_per_step": ms / steps, "mlups": nodes * steps / (ms * 1e-3) / 1e6,
             "achieved_gbs": bpn * nodes * steps / (ms * 1e-3) / 1e9, "bytes_per_node": bpn,
             "bulk_block": best, "bulk_rows": info["bulk_rows"], "general_rows": info["general_rows"],
-            "launches_per_step": info["launches_per_step"], "unstable_members": unstable,
+            "launches_per_step": info["launches_per_step"], "unstable_members": unstable, "ranks": ranks.world,
             "per_job_plain": {"value": base_sims, "unit": "sims/s", "jobs": baseline_jobs,
                               "mlups": base_nodes * steps / (per_job_ms * 1e-3) / 1e6},
             "speedup_vs_per_job": sims / base_sims}
@@ -363,16 +376,30 @@ def serving_leg(rate, n_jobs, storage="f32", baseline=True, graph_steps=0):
     import torch
 
     from wake_b200 import serve as S
+    from wake_b200.shard import Ranks, merge_served, shard
 
-    jobs = S.mixed_jobs(n_jobs, rate)
+    ranks = Ranks()
+
+    def whole(rep):
+        # N GPUs: each serves the jobs whose id is its rank mod N, on the same arrival clock
+        summ = rep.summary()
+        parts = ranks.gather({"jobs": summ["jobs"], "failed": summ["failed"], "makespan_s": rep.makespan,
+                              "node_steps": summ["node_steps"], "latencies_s": [r.latency for r in rep.results]})
+        if ranks.world > 1:
+            summ.update(merge_served(parts))
+        return summ
+
+    jobs = shard(S.mixed_jobs(n_jobs, rate), ranks.rank, ranks.world)
     free, _ = torch.cuda.mem_get_info()
     budget = int(0.8 * free)
+    ranks.barrier()
     rep = S.Server(budget, storage=storage, max_tick_steps=100, graph_steps=graph_steps).run(jobs, realtime=True)
-    out = {"rate_jobs_per_s": rate, "storage": storage, "graph_steps": graph_steps, **rep.summary()}
-    out["mlups"] = out["node_steps"] / max(rep.makespan, 1e-9) / 1e6
+    out = {"rate_jobs_per_s": rate, "storage": storage, "graph_steps": graph_steps, **whole(rep)}
+    out["mlups"] = out["node_steps"] / max(out["makespan_s"], 1e-9) / 1e6
     if baseline:
         torch.cuda.empty_cache()
-        base = S.run_per_job(jobs, storage=storage, realtime=True).summary()
+        ranks.barrier()
+        base = whole(S.run_per_job(jobs, storage=storage, realtime=True))
         out["per_job_plain"] = {k: base[k] for k in ("sims_per_s", "p50_latency_s", "p99_latency_s", "makespan_s",
                                                      "failed")}
         out["speedup_vs_per_job"] = out["sims_per_s"] / max(base["sims_per_s"], 1e-12)
@@ -678,7 +705,8 @@ def main():
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64; no dataset)",
                 "config": {"workload": WORKLOAD, "nodes": n_nodes, "storage": "f32",
                            "l2": "inputs larger than L2 (two 319 MB population buffers, 126 MB L2)",
-                           "parallelism": "replicas" if world > 1 else "single GPU",
+                           "parallelism": ("replicas of the sphere channel and the Taylor-Green cube; batched "
+                                           "sweep and served jobs split by job id mod N") if world > 1 else "single GPU",
                            "graph_steps": args.graph, "final_cd": cd},
                 "roofline": roof, "fp16": fp16, "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "taylor_green": tgv, "served": served,
                 "clocks": clocks.summary(),
