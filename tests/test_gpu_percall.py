@@ -232,3 +232,83 @@ def test_null_pointer_is_reported_not_faulted():
     wb.lib.d2q9_compute_macroscopic_moments(None, None, None, None, 16)
     assert wb.lib.wake_gpu_last_error_code() == -1
     wb.lib.wake_gpu_clear_error()
+
+
+# ----------------------------------------------------------------------------- ragged and empty inputs
+def _ref_lib():
+    import oracle
+
+    R = oracle.ref()
+    if R is None:
+        pytest.skip("reference build oracle/_ref is absent")
+    vp, F, I = C.c_void_p, C.c_float, C.c_int
+    R.d2q9_compute_macroscopic_moments.argtypes = [vp, vp, vp, vp, I]
+    R.d2q9_collide_bgk.argtypes = [vp, vp, vp, vp, vp, vp, F, F, F, I]
+    R.d3q19_collide_trt.argtypes = [vp, vp, vp, vp, vp, vp, vp, F, F, F, F, F, I]
+    return R
+
+
+def _pops(q, count, seed):
+    import oracle
+
+    rng = np.random.default_rng(seed)
+    rho = (1.0 + 0.01 * rng.standard_normal(count)).astype(np.float32)
+    u = [(0.03 * rng.standard_normal(count)).astype(np.float32) for _ in range(3)]
+    f = oracle.equilibrium(q, rho, u[0], u[1], u[2] if q != 9 else None, prec=32)
+    return np.ascontiguousarray((f * (1.0 + 0.01 * rng.standard_normal(f.shape))).astype(np.float32))
+
+
+@pytest.mark.parametrize("count", [1, 33, 257, 4099])
+def test_ragged_counts_match_reference(mode, count):
+    """Node counts that fill no whole block: the last block's tail must be neither skipped nor
+    overrun. Moments, BGK (D2Q9) and TRT (D3Q19) collide against the reference's kernels."""
+    R = _ref_lib()
+    A = Args(mode)
+    types = np.zeros(count, np.uint8)
+    types[::7] = 1  # some solids (copied through)
+    f9 = _pops(9, count, count)
+    want = [np.zeros(count, np.float32) for _ in range(3)]
+    R.d2q9_compute_macroscopic_moments(f9.ctypes.data, *[w.ctypes.data for w in want], count)
+    got = [A(np.full(count, np.nan, np.float32)) for _ in range(3)]
+    wb.lib.d2q9_compute_macroscopic_moments(A.ptr(A(f9)), *[A.ptr(g) for g in got], count)
+    for g, w in zip(got, want):
+        assert close(A.np(g), w)
+    fo_ref = np.zeros_like(f9)
+    mom = [np.zeros(count, np.float32) for _ in range(3)]
+    R.d2q9_collide_bgk(f9.ctypes.data, fo_ref.ctypes.data, types.ctypes.data, *[m.ctypes.data for m in mom], 0.7,
+                       0.0, 0.0, count)
+    fo = A(np.zeros_like(f9))
+    gm = [A(np.zeros(count, np.float32)) for _ in range(3)]
+    wb.lib.d2q9_collide_bgk(A.ptr(A(f9)), A.ptr(fo), A.ptr(A(types)), *[A.ptr(m) for m in gm], 0.7, 0.0, 0.0, count)
+    assert close(A.np(fo), fo_ref)
+    f19 = _pops(19, count, count + 1)
+    fo_ref = np.zeros_like(f19)
+    mom = [np.zeros(count, np.float32) for _ in range(4)]
+    R.d3q19_collide_trt(f19.ctypes.data, fo_ref.ctypes.data, types.ctypes.data, *[m.ctypes.data for m in mom], 0.75,
+                        1.3, 0.0, 0.0, 0.0, count)
+    fo = A(np.zeros_like(f19))
+    gm = [A(np.zeros(count, np.float32)) for _ in range(4)]
+    wb.lib.d3q19_collide_trt(A.ptr(A(f19)), A.ptr(fo), A.ptr(A(types)), *[A.ptr(m) for m in gm], 0.75, 1.3, 0.0,
+                             0.0, 0.0, count)
+    assert close(A.np(fo), fo_ref)
+
+
+def test_empty_inputs_touch_nothing(mode):
+    """Zero-sized calls (count 0, an extent of 0) return without writing, as the reference's
+    loops over empty ranges do, and record no error."""
+    A = Args(mode)
+    wb.lib.wake_gpu_clear_error()
+    sentinel = np.full(64, 7.0, np.float32)
+    bufs = [A(sentinel) for _ in range(6)]
+    t = A(np.zeros(64, np.uint8))
+    p = [A.ptr(b) for b in bufs]
+    wb.lib.d2q9_compute_macroscopic_moments(p[0], p[1], p[2], p[3], 0)
+    wb.lib.d2q9_collide_bgk(p[0], p[1], A.ptr(t), p[2], p[3], p[4], 0.7, 0.0, 0.0, 0)
+    wb.lib.d2q9_stream_periodic(p[0], p[1], 0, 4)
+    wb.lib.d3q19_stream_periodic(p[0], p[1], 4, 0, 2)
+    wb.lib.d3q19_apply_curved_bfl(p[0], p[1], None, None, None, None, None, None, 4, 4, 4, 0)
+    wb.lib.compute_vorticity_2d(p[0], p[1], p[2], 0, 8)
+    wb.lib.compute_vorticity_and_q_criterion_3d(p[0], p[1], p[2], p[3], p[4], p[5], p[5], 4, 4, 0)
+    for b in bufs:
+        assert np.array_equal(A.np(b), sentinel)
+    assert wb.lib.wake_gpu_last_error_code() == 0
