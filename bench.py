@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batch", action="store_true", help="skip the batched ellipse-sweep leg")
     p.add_argument("--batch-only", action="store_true", help="only the batched ellipse-sweep leg (one JSON line)")
+    p.add_argument("--batch-steps", type=int, default=0,
+                   help="with --batch-only: time this many steps instead of 5000 (a short run for ncu)")
     p.add_argument("--no-serve", action="store_true", help="skip the served-mix leg")
     p.add_argument("--no-tgv", action="store_true", help="skip the D3Q27 MRT Taylor-Green 384^3 leg")
     p.add_argument("--tgv-steps", type=int, default=5000, help="steps of the Taylor-Green leg (multiple of 500)")
@@ -592,7 +594,9 @@ def main():
         print(json.dumps(tgv_leg(L=args.tgv_size, steps=args.tgv_steps)))
         return
     if args.batch_only:
-        out = {"workload": BATCH_WORKLOAD, "f32": batched_leg("f32"), "f16": batched_leg("f16")}
+        # --batch-steps: a short run for profiling, with a proportionally short per-job baseline
+        kw = {"steps": args.batch_steps, "baseline_jobs": 2} if args.batch_steps else {}
+        out = {"workload": BATCH_WORKLOAD, "f32": batched_leg("f32", **kw), "f16": batched_leg("f16", **kw)}
         print(json.dumps(out))
         return
     world, rank, local = dist_setup(args)
