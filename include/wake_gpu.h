@@ -150,6 +150,17 @@ void thermal_compute_buoyancy_force_2d(const float temperature[], float gy_body[
                                        float g_gravity, int count);
 void thermal_apply_isothermal_wall(float g[], int nx, int ny, int y_wall, float t_wall);
 
+/* Immersed boundary, 2D: src/ispc/ibm_kernels.ispc:12-22 (velocity at the markers, Roma-Peskin
+ * 4-point delta, periodic in x) and 56-67 (marker forces times arc length spread onto the
+ * lattice body force; overlapping markers add atomically, so sums may differ from the
+ * reference's marker-order loop in the last bits). Called by ImmersedBoundary
+ * (src/ibm/immersed_boundary.cpp:87, 111). */
+void ibm_interpolate_velocity_2d(const float ux[], const float uy[], const float marker_x[], const float marker_y[],
+                                 float marker_ux[], float marker_uy[], int nx, int ny, int num_markers);
+void ibm_spread_force_2d(const float marker_x[], const float marker_y[], const float marker_fx[],
+                         const float marker_fy[], const float marker_ds[], float euler_gx[], float euler_gy[], int nx,
+                         int ny, int num_markers);
+
 /* Field analytics: src/ispc/analytics_kernels.ispc:4-10 (2D vorticity), 33-44
  * (3D vorticity vector + Q-criterion). Central differences with periodic wrap;
  * products and sums rounded in the reference's order without contraction.

@@ -394,7 +394,7 @@ def test_c2_sphere_channel_full_size_tracks_reference(golden):
     """C2 at full size and length in the form the reference can run: D3Q19 TRT (Lambda = 1/4),
     tau0 = 0.52, 256x128x128, sphere R = 12 with BFL links, x-periodic, y/z walls, 2000 steps.
     Fixture: the reference's own run (force history; rho and u on the planes z = 64 and y = 64
-    through the sphere) and the FP64 oracle's run of the same case. The GPU drag history stays
+    through the sphere, every other node) and the FP64 oracle's run of the same case. The GPU drag history stays
     within 1e-4 (relative L2) of the reference's; rho and u on both planes within 1e-5 of it, or
     within the reference's own distance to FP64 where that is larger; and the GPU is as close to
     FP64 as the reference."""
@@ -418,7 +418,7 @@ def test_c2_sphere_channel_full_size_tracks_reference(golden):
     planes = {}
     for k in ("rho", "ux", "uy", "uz"):
         a = m[k].reshape(c.nz, c.ny, c.nx)
-        planes[k] = np.concatenate([a[64].ravel(), a[:, 64, :].ravel()])
+        planes[k] = np.concatenate([a[64][::2, ::2].ravel(), a[:, 64, :][::2, ::2].ravel()])
     refp = {k: np.concatenate([d[f"ref_{k}_z64"].ravel(), d[f"ref_{k}_y64"].ravel()]) for k in planes}
     p64 = {k: np.concatenate([d[f"fp64_{k}_z64"].ravel(), d[f"fp64_{k}_y64"].ravel()]) for k in planes}
     comps = ("ux", "uy", "uz")

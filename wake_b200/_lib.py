@@ -67,6 +67,8 @@ _PROTOS = {
     "thermal_collide_d2q9": (None, [vp, vp, vp, vp, vp, vp, F, I]),
     "thermal_compute_buoyancy_force_2d": (None, [vp, vp, F, F, F, I]),
     "thermal_apply_isothermal_wall": (None, [vp, I, I, I, F]),
+    "ibm_interpolate_velocity_2d": (None, [vp, vp, vp, vp, vp, vp, I, I, I]),
+    "ibm_spread_force_2d": (None, [vp, vp, vp, vp, vp, vp, vp, I, I, I]),
     "compute_vorticity_2d": (None, [vp, vp, vp, I, I]),
     "compute_vorticity_and_q_criterion_3d": (None, [vp, vp, vp, vp, vp, vp, vp, I, I, I]),
     # fused engine

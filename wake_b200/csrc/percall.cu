@@ -764,6 +764,67 @@ extern "C" int d3q19_compute_momentum_exchange_forces_noalloc(const float f_post
     return WAKE_OK;
 }
 
+// ---------------------------------------------------------------- immersed boundary (2D)
+// Roma-Peskin 4-point regularised delta, one dimension (src/ispc/ibm_kernels.ispc:3-8).
+__device__ __forceinline__ float peskin_1d(float r) {
+    const float a = fabsf(r);
+    if (a >= 2.0f) return 0.0f;
+    return 0.25f * (1.0f + cosf(0.5f * 3.14159265358979323846f * a));
+}
+
+__device__ __forceinline__ int wrap_x(int px, int nx) { return (px % nx + nx) % nx; }
+
+// Velocity at each marker: the 5 x 5 lattice neighbourhood weighted by the delta kernel,
+// periodic in x, rows outside [0, ny) skipped (ibm_kernels.ispc:12-52). Thread per marker.
+__global__ void k_ibm_interpolate(const float* __restrict__ ux, const float* __restrict__ uy,
+                                  const float* __restrict__ mx_, const float* __restrict__ my_,
+                                  float* __restrict__ mux, float* __restrict__ muy, int nx, int ny, int n) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    const float mx = mx_[m], my = my_[m];
+    const int fx = static_cast<int>(floorf(mx)), fy = static_cast<int>(floorf(my));
+    float iu = 0.0f, iv = 0.0f;
+    for (int iy = -2; iy <= 2; ++iy) {
+        const int py = fy + iy;
+        if (py < 0 || py >= ny) continue;
+        const float wy = peskin_1d(static_cast<float>(py) - my);
+        const long long row = static_cast<long long>(py) * nx;
+        for (int ix = -2; ix <= 2; ++ix) {
+            const int px = fx + ix;
+            const float w = peskin_1d(static_cast<float>(px) - mx) * wy;
+            const long long e = row + wrap_x(px, nx);
+            iu += w * ux[e];
+            iv += w * uy[e];
+        }
+    }
+    mux[m] = iu;
+    muy[m] = iv;
+}
+
+// Force spreading (ibm_kernels.ispc:56-99): marker force times its arc length onto the 5 x 5
+// neighbourhood, x weight from the delta kernel, y weight 0.25 (1 + cos(pi |py - my| / 2))
+// without the kernel's |r| < 2 cut-off, as the reference computes it. One thread per (marker,
+// stencil point); overlapping markers add with atomics, so sums may differ from the reference's
+// marker-order loop in the last bits.
+__global__ void k_ibm_spread(const float* __restrict__ mx_, const float* __restrict__ my_,
+                             const float* __restrict__ mfx, const float* __restrict__ mfy,
+                             const float* __restrict__ mds, float* __restrict__ gx, float* __restrict__ gy, int nx,
+                             int ny, int n) {
+    const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (t >= 25ll * n) return;
+    const int m = static_cast<int>(t / 25), k = static_cast<int>(t % 25);
+    const float mx = mx_[m], my = my_[m];
+    const int py = static_cast<int>(floorf(my)) - 2 + k / 5;
+    if (py < 0 || py >= ny) return;
+    const int px = static_cast<int>(floorf(mx)) - 2 + k % 5;
+    const float fx = mfx[m] * mds[m], fy = mfy[m] * mds[m];
+    const float wy = 0.25f * (1.0f + cosf(0.5f * 3.14159265358979323846f * fabsf(static_cast<float>(py) - my)));
+    const float w = peskin_1d(static_cast<float>(px) - mx) * wy;
+    const long long e = static_cast<long long>(py) * nx + wrap_x(px, nx);
+    atomicAdd(gx + e, w * fx);
+    atomicAdd(gy + e, w * fy);
+}
+
 extern "C" {
 
 void d3q19_apply_curved_bfl(float f_dst[], const float f_src[], const int fluid_indices[], const int q_dirs[],
@@ -820,6 +881,46 @@ void thermal_apply_isothermal_wall(float g[], int nx, int ny, int y_wall, float 
     s.inout(g, 9 * static_cast<std::size_t>(nx) * ny);
     if (s.begin()) return;
     k_isothermal_wall<<<blocks_for(nx, 128), 128>>>(s.ptr<float>(0), nx, ny, y_wall, t_wall);
+    s.end();
+}
+
+// src/ispc/ibm_kernels.ispc:12-22
+void ibm_interpolate_velocity_2d(const float ux[], const float uy[], const float marker_x[], const float marker_y[],
+                                 float marker_ux[], float marker_uy[], int nx, int ny, int num_markers) {
+    if (num_markers <= 0 || nx <= 0 || ny <= 0) return;
+    const std::size_t n = static_cast<std::size_t>(nx) * ny, nm = static_cast<std::size_t>(num_markers);
+    Stager s;
+    s.in(ux, n);
+    s.in(uy, n);
+    s.in(marker_x, nm);
+    s.in(marker_y, nm);
+    s.full_out(marker_ux, nm);
+    s.full_out(marker_uy, nm);
+    if (s.begin()) return;
+    k_ibm_interpolate<<<blocks_for(num_markers, 128), 128>>>(s.ptr<float>(0), s.ptr<float>(1), s.ptr<float>(2),
+                                                             s.ptr<float>(3), s.ptr<float>(4), s.ptr<float>(5), nx,
+                                                             ny, num_markers);
+    s.end();
+}
+
+// src/ispc/ibm_kernels.ispc:56-67
+void ibm_spread_force_2d(const float marker_x[], const float marker_y[], const float marker_fx[],
+                         const float marker_fy[], const float marker_ds[], float euler_gx[], float euler_gy[], int nx,
+                         int ny, int num_markers) {
+    if (num_markers <= 0 || nx <= 0 || ny <= 0) return;
+    const std::size_t n = static_cast<std::size_t>(nx) * ny, nm = static_cast<std::size_t>(num_markers);
+    Stager s;
+    s.in(marker_x, nm);
+    s.in(marker_y, nm);
+    s.in(marker_fx, nm);
+    s.in(marker_fy, nm);
+    s.in(marker_ds, nm);
+    s.inout(euler_gx, n);
+    s.inout(euler_gy, n);
+    if (s.begin()) return;
+    k_ibm_spread<<<blocks_for(25ll * num_markers, 256), 256>>>(s.ptr<float>(0), s.ptr<float>(1), s.ptr<float>(2),
+                                                               s.ptr<float>(3), s.ptr<float>(4), s.ptr<float>(5),
+                                                               s.ptr<float>(6), nx, ny, num_markers);
     s.end();
 }
 
