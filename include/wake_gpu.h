@@ -256,7 +256,8 @@ int wake_grid_set_populations_device(wake_grid* g, const float* f_dev /* device 
 int wake_grid_enable_forces(wake_grid* g, float cx, float cy, float cz, float r_max, int history_capacity);
 int wake_grid_disable_forces(wake_grid* g);
 /* Copies up to max records, oldest first, of the last min(steps, capacity)
- * steps; returns the number copied or a negative error. */
+ * steps into a host or device buffer (only those records cross the bus);
+ * returns the number copied or a negative error. */
 int wake_grid_get_force_history(wake_grid* g, double* out /* [max][3] */, int max);
 /* Number of steps recorded since forces were enabled. */
 long long wake_grid_force_count(wake_grid* g);

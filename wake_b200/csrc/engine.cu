@@ -1275,16 +1275,19 @@ int wake_grid_get_force_history(wake_grid* g, double* out, int max) {
     if (!g->mem_on) return 0;
     const long long count = wake_grid_force_count(g);
     if (count < 0) return static_cast<int>(count);
-    std::vector<double> ring(3 * static_cast<std::size_t>(g->hist_cap));
-    WK_CUDA(cudaMemcpyAsync(ring.data(), g->d_hist.p, sizeof(double) * ring.size(), cudaMemcpyDeviceToHost, g->stream));
+    // the oldest step still in the ring, then at most `max` steps in order: one or two
+    // contiguous runs of the ring, copied straight into the caller's buffer
+    const long long cap = g->hist_cap;
+    const long long first = std::max(0ll, count - cap);
+    const long long n = std::min(count, first + static_cast<long long>(max)) - first;
+    if (n <= 0) return 0;
+    const long long s0 = first % cap, run1 = std::min(n, cap - s0);
+    const double* ring = g->d_hist.as<double>();
+    WK_CUDA(cudaMemcpyAsync(out, ring + 3 * s0, sizeof(double) * 3 * run1, cudaMemcpyDefault, g->stream));
+    if (n > run1)
+        WK_CUDA(cudaMemcpyAsync(out + 3 * run1, ring, sizeof(double) * 3 * (n - run1), cudaMemcpyDefault, g->stream));
     WK_CUDA(cudaStreamSynchronize(g->stream));
-    const long long first = std::max(0ll, count - g->hist_cap);
-    int n = 0;
-    for (long long s = first; s < count && n < max; ++s, ++n) {
-        const long long slot = s % g->hist_cap;
-        for (int c = 0; c < 3; ++c) out[3 * n + c] = ring[3 * slot + c];
-    }
-    return n;
+    return static_cast<int>(n);
 }
 
 int wake_grid_step(wake_grid* g, int n, float gx, float gy, float gz) {
