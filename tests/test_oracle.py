@@ -2,16 +2,16 @@
 outputs (golden fixtures and, where built, the reference library), and the
 analytic properties of the pieces the reference lacks. CPU only."""
 import re
-from pathlib import Path
 
 import numpy as np
 import pytest
 
 import oracle
 from conftest import rel_l2, vel_rel_l2
+from oracle.build_ref import reference_dir
 from wake_b200 import workloads as W
 
-REF_SRC = Path("/root/reference")
+REF_SRC = reference_dir()
 
 
 def eq(q, rho, u):
