@@ -114,6 +114,9 @@ int build_rows(wake_batch* b) {
     layout.reserve(b->members.size());
     for (const auto& m : b->members) layout.emplace_back(m.g, m.g->geom_version);
     if (layout == b->layout && b->gen_first.size() == b->members.size()) return WAKE_OK;
+    // queued steps may still read the old lists: let them finish, then lists can move freely
+    WK_CUDA(cudaStreamSynchronize(b->stream));
+    if (b->side) WK_CUDA(cudaStreamSynchronize(b->side));
     std::vector<uint4> fast, tiles, gen4, mixed;
     std::vector<uint2> gen;
     b->gen_first.assign(b->members.size(), 0);
@@ -127,13 +130,13 @@ int build_rows(wake_batch* b) {
         for (uint4 t : g->h_gen4) gen4.push_back(make_uint4(m, t.y, t.z, 0u));
         for (uint4 sp : g->h_mixed) mixed.push_back(make_uint4(m, sp.y, sp.z, sp.w));
     }
-    WK_CUDA(b->d_mixed.ensure(sizeof(uint4) * std::max<std::size_t>(1, mixed.size())));
+    WK_CUDA(b->d_mixed.grow(sizeof(uint4) * std::max<std::size_t>(1, mixed.size())));
     if (!mixed.empty())
         WK_CUDA(cudaMemcpyAsync(b->d_mixed.p, mixed.data(), sizeof(uint4) * mixed.size(), cudaMemcpyHostToDevice,
                                 b->stream));
     b->n_mixed = static_cast<int>(mixed.size());
-    WK_CUDA(b->d_tiles.ensure(sizeof(uint4) * std::max<std::size_t>(1, tiles.size())));
-    WK_CUDA(b->d_gen4.ensure(sizeof(uint4) * std::max<std::size_t>(1, gen4.size())));
+    WK_CUDA(b->d_tiles.grow(sizeof(uint4) * std::max<std::size_t>(1, tiles.size())));
+    WK_CUDA(b->d_gen4.grow(sizeof(uint4) * std::max<std::size_t>(1, gen4.size())));
     if (!tiles.empty())
         WK_CUDA(cudaMemcpyAsync(b->d_tiles.p, tiles.data(), sizeof(uint4) * tiles.size(), cudaMemcpyHostToDevice,
                                 b->stream));
@@ -142,8 +145,8 @@ int build_rows(wake_batch* b) {
                                 b->stream));
     b->n_tiles = static_cast<int>(tiles.size());
     b->n_tile_gen = static_cast<int>(gen4.size());
-    WK_CUDA(b->d_fast.ensure(sizeof(uint4) * std::max<std::size_t>(1, fast.size())));
-    WK_CUDA(b->d_gen.ensure(sizeof(uint2) * std::max<std::size_t>(1, gen.size())));
+    WK_CUDA(b->d_fast.grow(sizeof(uint4) * std::max<std::size_t>(1, fast.size())));
+    WK_CUDA(b->d_gen.grow(sizeof(uint2) * std::max<std::size_t>(1, gen.size())));
     if (!fast.empty())
         WK_CUDA(cudaMemcpyAsync(b->d_fast.p, fast.data(), sizeof(uint4) * fast.size(), cudaMemcpyHostToDevice, b->stream));
     if (!gen.empty())
@@ -198,11 +201,13 @@ int build_tables(wake_batch* b) {
     const bool same_red = red.size() == b->up_red.size() &&
                           (red.empty() || std::memcmp(red.data(), b->up_red.data(), sizeof(MemRed) * red.size()) == 0);
     if (same_dom && same_red) return WAKE_OK;
+    WK_CUDA(cudaStreamSynchronize(b->stream));  // queued steps may still read the old tables
+    if (b->side) WK_CUDA(cudaStreamSynchronize(b->side));
     const void* old_dom = b->d_dom.p;
     const void* old_red = b->d_red.p;
     const int old_nred = b->n_red;
-    WK_CUDA(b->d_dom.ensure(sizeof(BatchDom) * std::max<std::size_t>(1, n)));
-    WK_CUDA(b->d_red.ensure(sizeof(MemRed) * std::max<std::size_t>(1, red.size())));
+    WK_CUDA(b->d_dom.grow(sizeof(BatchDom) * std::max<std::size_t>(1, n)));
+    WK_CUDA(b->d_red.grow(sizeof(MemRed) * std::max<std::size_t>(1, red.size())));
     if (n) WK_CUDA(cudaMemcpyAsync(b->d_dom.p, dom.data(), sizeof(BatchDom) * n, cudaMemcpyHostToDevice, b->stream));
     if (!red.empty())
         WK_CUDA(cudaMemcpyAsync(b->d_red.p, red.data(), sizeof(MemRed) * red.size(), cudaMemcpyHostToDevice, b->stream));

@@ -65,6 +65,13 @@ struct DevMem {
         p = nullptr;
         bytes = 0;
     }
+    // Grow to at least b bytes when no queued work can still use the current block: the old
+    // block goes back to the cache instead of a cudaFree (which would wait for the whole device).
+    cudaError_t grow(std::size_t b) {
+        if (p && bytes >= b) return cudaSuccess;
+        release();
+        return ensure(b);
+    }
     // (Re)allocate when the current block is smaller than b. Returns cudaSuccess or the error.
     cudaError_t ensure(std::size_t b) {
         if (p && bytes >= b) return cudaSuccess;

@@ -1574,20 +1574,23 @@ int wake_grid_release_scratch(wake_grid* g) {
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
     const int r = prepare(g);  // a pending re-collide consumes the FP32 populations first
     if (r) return r;
+    // every queued use of the scratch has finished, so its blocks go back to the process cache:
+    // no cudaFree, which would wait for the whole device (other lattices' steps included)
     WK_CUDA(cudaStreamSynchronize(g->stream));
-    g->m_f.reset();
+    if (g->side) WK_CUDA(cudaStreamSynchronize(g->side));
+    g->m_f.release();
     g->mf_valid = false;
     if (g->k > 0 || !g->pending) {  // the initial temperature populations were collided already
-        g->m_t.reset();
+        g->m_t.release();
         g->mt_valid = false;
     }
-    g->m_an.reset();
-    g->m_rho.reset();
-    g->m_ux.reset();
-    g->m_uy.reset();
-    g->m_uz.reset();
-    g->m_speed.reset();
-    g->m_diag.reset();
+    g->m_an.release();
+    g->m_rho.release();
+    g->m_ux.release();
+    g->m_uy.release();
+    g->m_uz.release();
+    g->m_speed.release();
+    g->m_diag.release();
     return WAKE_OK;
 }
 
