@@ -70,7 +70,8 @@ def parse():
                    help="profiling mode: only warm-up + timed steps of this storage, plain launches, one JSON line "
                         "('vorticity': --steps calls of the 3D vorticity / Q-criterion kernel on 256^3 device fields)")
     p.add_argument("--block", type=int, default=0, help="threads per block of the fused step (0: automatic)")
-    p.add_argument("--kernel", type=int, default=0, help="pure-gather row kernel: 0 auto, 1 direct gather, 2 staged")
+    p.add_argument("--kernel", type=int, default=0,
+                   help="pure-gather kernel: 0 auto, 1 spans, 2 staged tiles, 3 whole rows, 4 pipelined whole rows")
     return p.parse_args()
 
 
@@ -240,6 +241,8 @@ def timed_steps(g, case, steps, warmup, world):
     stream = torch.cuda.Stream()  # a real stream handle: the legacy default stream is 0
     g.set_stream(stream.cuda_stream)
     g.step(case.collision, use_les=case.les, smag_const=case.cs_smag, n=warmup)
+    # the step graph (if any) is captured and instantiated here, outside the timed region
+    g.prepare_steps(case.collision, use_les=case.les, smag_const=case.cs_smag)
     torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()
@@ -510,12 +513,32 @@ def tgv_leg(L=384, steps=5000, every=500, graph=20):
     return out
 
 
-def reference_sample(case_ref, steps_cap, budget_s, threads=1):
-    """Time the reference's own LatticeGrid3D::step + momentum exchange (oracle/_ref) on host cores."""
+def load_workloads():
+    """wake_b200/workloads.py loaded by path: its case builders are numpy only, and importing the
+    wake_b200 package would load libwake_b200.so into a process that must not use it."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("wake_workloads_np", ROOT / "wake_b200" / "workloads.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod  # dataclasses look their module up while the file executes
+    spec.loader.exec_module(mod)
+    return mod
+
+
+REFERENCE_VARIANT = ("the reference's own LatticeGrid3D::step + momentum exchange (oracle/_ref: its host classes and "
+                     "its kernels translated mechanically from ISPC) on the same 256x128x128 sphere channel, TRT, "
+                     "tau0=0.52, BFL links, momentum exchange every step, in the form the reference can express: "
+                     "x-periodic, y/z half-way walls, no Zou-He (the reference has no 3D Zou-He), Smagorinsky tau "
+                     "computed but not applied (the reference discards it)")
+
+
+def reference_sample(case_ref, steps, warmup, budget_s, threads=1):
+    """Time the reference's own LatticeGrid3D::step + momentum exchange (oracle/_ref) on host cores:
+    `threads` independent replicas (the reference is single-threaded), `warmup` untimed steps each,
+    then `steps` timed steps each, fewer if they would not fit `budget_s` at the warm-up's pace."""
     import oracle
 
     L = oracle.ref()
-    kind = "reference"
     if L is None:
         return None
     c = case_ref
@@ -527,35 +550,43 @@ def reference_sample(case_ref, steps_cap, budget_s, threads=1):
         L.ref3d_set_solid_sphere(gr._h, *c.sphere)
         L.ref3d_build_curved_sphere_links(gr._h, *c.sphere)
         grids.append(gr)
-    # one warm-up step, then as many steps as fit in the budget
-    t0 = time.perf_counter()
-    grids[0].step_forces(1, c.collision, c.mem[:3], c.mem[3], use_les=True, cs=c.cs_smag)
-    t_step = time.perf_counter() - t0
-    n = int(max(1, min(steps_cap, budget_s // max(t_step, 1e-6))))
 
-    def run(gr):
+    def run(gr, n):
         gr.step_forces(n, c.collision, c.mem[:3], c.mem[3], use_les=True, cs=c.cs_smag)
 
-    ths = [threading.Thread(target=run, args=(gr,)) for gr in grids]
-    t0 = time.perf_counter()
-    for t in ths:
-        t.start()
-    for t in ths:
-        t.join()
-    dt = time.perf_counter() - t0
+    def parallel(n):
+        ths = [threading.Thread(target=run, args=(gr, n)) for gr in grids]
+        t0 = time.perf_counter()
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        return time.perf_counter() - t0
+
+    t_warm = parallel(max(1, warmup))
+    t_step = t_warm / max(1, warmup)
+    n = int(max(1, min(steps, budget_s // max(t_step, 1e-6))))
+    dt = parallel(n)
     mlups = threads * c.n * n / dt / 1e6
-    return {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": kind,
-            "sample": f"{n} reference steps of the {c.nx}x{c.ny}x{c.nz} sphere channel (x-periodic, y/z walls, "
-                      f"TRT, LES flag on, BFL, momentum exchange per step){' x ' + str(threads) + ' replicas' if threads > 1 else ''}",
-            "seconds": dt, "steps": n}
+    return {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": "reference",
+            "sample": f"{n} timed steps after {max(1, warmup)} untimed, on each of {threads} independent replica(s) "
+                      f"of {REFERENCE_VARIANT}",
+            "seconds": dt, "steps": n, "per_core_mlups": mlups / threads}
+
+
+def workload_config(n_nodes, world):
+    """The `config` of both arms' JSON lines (the workload, not run results)."""
+    return {"workload": WORKLOAD, "nodes": n_nodes, "storage": "f32",
+            "l2": "inputs larger than L2 (two 319 MB population buffers, 126 MB L2)",
+            "parallelism": ("replicas of the sphere channel and the Taylor-Green cube; batched sweep and served jobs "
+                            "split by job id mod N") if world > 1 else "single GPU"}
 
 
 def run_reference_impl(args):
-    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    world, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from wake_b200 import workloads as W
-
+    W = load_workloads()
     c = W.sphere_channel(reference_variant=True, collision=1, les=False)
     try:
         import psutil
@@ -564,18 +595,21 @@ def run_reference_impl(args):
     except Exception:
         mem_cap = 4
     threads = max(1, min(os.cpu_count() or 1, 32, mem_cap))
-    res = reference_sample(c, steps_cap=max(1, args.steps), budget_s=90.0, threads=threads)
+    res = reference_sample(c, steps=max(1, args.steps), warmup=max(1, args.warmup), budget_s=120.0, threads=threads)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libwake_ref.so missing"}))
         return
     ms = res["seconds"] * 1e3 / res["steps"]
     line = {"impl": "reference", "metric": "MLUPS", "value": res["value"], "unit": "MLUPS", "n_gpus": args.gpus,
-            "steps": res["steps"], "warmup": 1, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64)",
-            "config": {"workload": WORKLOAD + " [reference-expressible variant: x-periodic, y/z walls, no Zou-He, "
-                                                "LES computed but not applied]", "nodes": c.n},
+            "steps": res["steps"], "warmup": max(1, args.warmup), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64; no dataset)",
+            "config": workload_config(c.n, world),
+            "reference_variant": REFERENCE_VARIANT,
+            "per_core_mlups": res["per_core_mlups"],
             "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": res["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if res["steps"] < args.steps:
+        line["steps_requested"] = args.steps
     print(json.dumps(line))
 
 
@@ -709,7 +743,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         c_ref = W.sphere_channel(reference_variant=True, collision=1, les=False)
-        res = reference_sample(c_ref, steps_cap=40, budget_s=20.0, threads=1)
+        res = reference_sample(c_ref, steps=40, warmup=1, budget_s=20.0, threads=1)
         if res is not None:
             cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
@@ -718,11 +752,7 @@ def main():
         line = {"metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64; no dataset)",
-                "config": {"workload": WORKLOAD, "nodes": n_nodes, "storage": "f32",
-                           "l2": "inputs larger than L2 (two 319 MB population buffers, 126 MB L2)",
-                           "parallelism": ("replicas of the sphere channel and the Taylor-Green cube; batched "
-                                           "sweep and served jobs split by job id mod N") if world > 1 else "single GPU",
-                           "graph_steps": args.graph, "final_cd": cd},
+                "config": workload_config(n_nodes, world), "graph_steps": args.graph, "final_cd": cd,
                 "roofline": roof, "fp16": fp16, "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "taylor_green": tgv, "served": served,
                 "clocks": clocks.summary(),
                 "gpu_launches": launches_per_step * args.steps}

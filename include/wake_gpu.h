@@ -128,11 +128,20 @@ void d3q19_compute_momentum_exchange_forces(const float f_post_collision[], cons
  * per-block partial sums in a fixed 384 KiB device array of the library (held by
  * every GPU that loads the library until the process exits), which limits the
  * lattice to nx*ny*nz <= 4,194,304 nodes; larger sizes are rejected with
- * WAKE_ERR_INVALID. Every pointer must be device or managed memory (host
- * buffers would need allocated staging). Returns 0 or a WAKE_ERR_* code, and
- * returns after the result is written. The first call on each device looks up
- * the array's device address (once per device); make that first call before any
- * stream capture. All calls share the array: calls that overlap on the GPU race. */
+ * WAKE_ERR_INVALID. Every pointer must be memory of the current GPU or managed
+ * memory (host buffers would need allocated staging). The buffers use the
+ * reference's unpadded layout, f [19][nx*ny*nz] and cell_type [nx*ny*nz], with
+ * the populations the reference passes (its f_src after a step); a resident
+ * lattice's state buffers are padded per plane and hold post-collision values,
+ * so pass what wake_grid_get_populations writes instead. The kernels run on the
+ * legacy default stream and the call returns after cudaStreamSynchronize(0):
+ * inputs written on other streams (a resident grid's or batch's streams do not
+ * synchronise with the legacy stream) must be complete before the call. Returns
+ * 0 or a WAKE_ERR_* code. The first call on each device looks up the array's
+ * device address (once per device); make that first call before any stream
+ * capture. All calls share the array: calls that overlap on the GPU race. The
+ * partial sums are added in another order than the allocating entry point's
+ * above 303,104 nodes, so the two agree to FP64 rounding there, not bit for bit. */
 int d3q19_compute_momentum_exchange_forces_noalloc(const float f_post_collision[], const uint8_t cell_type[], int nx,
                                                    int ny, int nz, float center_x, float center_y, float center_z,
                                                    float max_radius, float* fx_out, float* fy_out, float* fz_out);
@@ -267,6 +276,13 @@ int wake_grid_step(wake_grid* g, int n, float gx, float gy, float gz);
 /* Capture n steps in a CUDA graph (replayed by wake_grid_step whenever n is a
  * multiple of the captured count and nothing was reconfigured). 0 disables. */
 int wake_grid_use_graph(wake_grid* g, int steps_per_graph);
+/* Do now the one-time work that the next wake_grid_step with this body force
+ * would do first: re-collide after a parameter or geometry change and, when a
+ * graph size is set, capture and instantiate the graph from the current buffer
+ * parity. Advances nothing; returns after that work has finished, so that a
+ * timed run of wake_grid_step measures the steps alone. No reference
+ * counterpart. */
+int wake_grid_prepare_steps(wake_grid* g, float gx, float gy, float gz);
 long long wake_grid_step_count(wake_grid* g);
 /* Block until the grid's stream is idle; reports device-side numeric errors. */
 int wake_grid_synchronize(wake_grid* g);

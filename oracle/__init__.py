@@ -108,6 +108,7 @@ def ref() -> C.CDLL | None:
             "ref2d_step_forces": (None, [vp, I, F, F, I, F, I, F, F, F, vp]),
             "ref2d_get_f": (None, [vp, vp]), "ref2d_get_macro": (None, [vp, vp, vp, vp, vp]),
             "ref2d_get_cell_types": (None, [vp, vp]), "ref2d_total_mass": (F, [vp]),
+            "ref2d_total_ke": (F, [vp]), "ref2d_max_speed": (F, [vp]),
             "ref3d_create": (vp, [I, I, I, F]), "ref3d_destroy": (None, [vp]),
             "ref3d_init_fields": (None, [vp, vp, vp, vp, vp]), "ref3d_set_periodic": (None, [vp, I]),
             "ref3d_set_cell_type": (None, [vp, I, I, I, I]), "ref3d_set_solid_sphere": (None, [vp, F, F, F, F]),
@@ -118,7 +119,8 @@ def ref() -> C.CDLL | None:
             "ref3d_get_f": (None, [vp, vp]), "ref3d_get_macro": (None, [vp, vp, vp, vp, vp, vp]),
             "ref3d_get_cell_types": (None, [vp, vp]), "ref3d_num_links": (I, [vp]),
             "ref3d_get_links": (None, [vp, vp, vp, vp]), "ref3d_is_periodic": (I, [vp]),
-            "ref3d_total_mass": (F, [vp]), "ref_strouhal_frequency": (F, [vp, I, F]),
+            "ref3d_total_mass": (F, [vp]), "ref3d_total_ke": (F, [vp]), "ref3d_max_speed": (F, [vp]),
+            "ref_strouhal_frequency": (F, [vp, I, F]),
             "ref_vtk_export_2d": (I, [vp, C.c_char_p, vp]), "ref_vtk_export_3d": (I, [vp, C.c_char_p, vp, vp]),
             "ref_vtk_pvd": (I, [C.c_char_p, C.c_char_p, I, I, I, F]),
             "compute_vorticity_2d": (None, [vp, vp, vp, I, I]),

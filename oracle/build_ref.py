@@ -51,7 +51,10 @@ FOREACH = re.compile(r"foreach\s*\(\s*(\w+)\s*=\s*(.+?)\s*\.\.\.\s*(.+?)\s*\)\s*
 
 
 def reference_dir() -> Path:
-    return Path(os.environ.get("WAKE_REFERENCE_DIR", "/root/reference"))
+    """The reference checkout: WAKE_REFERENCE_DIR, else a directory named `reference` beside
+    the one that holds this repository."""
+    env = os.environ.get("WAKE_REFERENCE_DIR")
+    return Path(env) if env else Path(__file__).resolve().parents[2] / "reference"
 
 
 def translate(text: str) -> str:

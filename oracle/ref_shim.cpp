@@ -178,6 +178,7 @@ void ref3d_get_links(void* h, int* idx, int* q, float* delta) {
 int ref3d_is_periodic(void* h) { return static_cast<LatticeGrid3D*>(h)->is_periodic() ? 1 : 0; }
 float ref3d_total_mass(void* h) { return static_cast<LatticeGrid3D*>(h)->compute_total_mass(); }
 float ref3d_total_ke(void* h) { return static_cast<LatticeGrid3D*>(h)->compute_total_kinetic_energy(); }
+float ref3d_max_speed(void* h) { return static_cast<LatticeGrid3D*>(h)->compute_max_speed(); }
 
 // ---------------------------------------------------------------- Strouhal FFT
 // ---------------------------------------------------------------- telemetry files

@@ -45,10 +45,35 @@
 #include <cmath>
 #include <complex>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 namespace {
+
+// Runs fn(begin, end) over [0, n) split into contiguous ranges on host threads
+// (WAKE_ORACLE_THREADS, default: every hardware thread). Used only for loops
+// whose iterations write disjoint outputs and read nothing another iteration
+// writes, so the result does not depend on the thread count.
+template <class Fn>
+void parallel_ranges(std::size_t n, Fn&& fn) {
+    unsigned t = std::thread::hardware_concurrency();
+    if (const char* e = std::getenv("WAKE_ORACLE_THREADS")) t = static_cast<unsigned>(std::max(1, std::atoi(e)));
+    t = std::max(1u, std::min<unsigned>(t, 64u));
+    if (t == 1 || n < 4096) {
+        fn(std::size_t(0), n);
+        return;
+    }
+    const std::size_t chunk = (n + t - 1) / t;
+    std::vector<std::thread> pool;
+    for (unsigned k = 0; k < t; ++k) {
+        const std::size_t b = k * chunk, e = std::min(n, b + chunk);
+        if (b >= e) break;
+        pool.emplace_back([&fn, b, e] { fn(b, e); });
+    }
+    for (auto& th : pool) th.join();
+}
 
 enum Cell : uint8_t { FLUID = 0, SOLID = 1, INFLOW = 2, OUTFLOW = 3, MOVING_WALL = 6 };
 
@@ -547,7 +572,8 @@ struct Grid {
     void step() {
         const int Q = L::Q;
         // 1-2. collide f_src -> f_dst; solid nodes copy through (d2q9_collision_bgk.ispc:22-28)
-        for (std::size_t i = 0; i < n; ++i) {
+        parallel_ranges(n, [&](std::size_t i0, std::size_t i1) {
+        for (std::size_t i = i0; i < i1; ++i) {
             R f[L::Q], o[L::Q], r, u[3];
             for (int q = 0; q < Q; ++q) f[q] = fsrc[q * n + i];
             if (type[i] == SOLID) {
@@ -573,6 +599,7 @@ struct Grid {
             }
             for (int q = 0; q < Q; ++q) fdst[q * n + i] = o[q];
         }
+        });
         if (thermal_on())
             for (std::size_t i = 0; i < n; ++i)
                 if (type[i] == SOLID)
@@ -584,8 +611,9 @@ struct Grid {
             const R cuw = R(L::cx[q]) * R(p.u_wall[0]) + R(L::cy[q]) * R(p.u_wall[1]) + R(L::cz[q]) * R(p.u_wall[2]);
             mom[q] = R(2) * wq<L, R>(q) * R(3) * cuw;
         }
-        for (int z = 0; z < nz; ++z)
-            for (int y = 0; y < ny; ++y)
+        parallel_ranges(std::size_t(nz) * ny, [&](std::size_t r0, std::size_t r1) {
+        for (std::size_t row = r0; row < r1; ++row) {
+            const int z = static_cast<int>(row / ny), y = static_cast<int>(row % ny);
                 for (int x = 0; x < nx; ++x) {
                     const std::size_t i = at(x, y, z);
                     for (int q = 0; q < Q; ++q) {
@@ -601,6 +629,8 @@ struct Grid {
                         else fsrc[q * n + i] = fdst[q * n + s];
                     }
                 }
+        }
+        });
         // 3b. temperature: pull, anti-bounce-back through the y walls, bounce-back at solids
         if (thermal_on()) {
             for (int y = 0; y < ny; ++y)
@@ -688,7 +718,8 @@ struct Grid {
     }
 
     void refresh_macro() {
-        for (std::size_t i = 0; i < n; ++i) {
+        parallel_ranges(n, [&](std::size_t i0, std::size_t i1) {
+        for (std::size_t i = i0; i < i1; ++i) {
             R g[3] = {R(p.g[0]), R(p.g[1]), R(p.g[2])};
             if (thermal_on()) g[1] += R(p.beta_g) * (temperature(i) - R(p.t_ref));
             R f[L::Q], r, u[3];
@@ -700,6 +731,7 @@ struct Grid {
             uz[i] = u[2];
             speed[i] = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
         }
+        });
     }
 
     // Momentum exchange on f_src (forces_momentum_exchange.ispc:6-138): fluid nodes only,

@@ -343,6 +343,85 @@ def c2_case(R, steps=2000):
          **{f"ref_{k}": v for k, v in ref_planes.items()}, **{f"fp64_{k}": v for k, v in o_planes.items()})
 
 
+C3_EDGE, C3_EVERY, C3_STEPS, C3_SUB = 96, 500, 5000, 3
+
+
+def c3_case(edge=C3_EDGE, steps=C3_STEPS, every=C3_EVERY, sub=C3_SUB):
+    """The C3 Taylor-Green vortex (D3Q27 MRT, u0 = 0.04, tau = 0.51, 5000 steps) on an edge^3
+    periodic cube, in the FP64 oracle only: the reference has no D3Q27 MRT, so FP64 is the
+    yardstick of the FP32 / FP16 / BF16 storages. The start is the equilibrium of the float32
+    fields, rounded to float32 (the GPU's initial state). Every `every` steps: the FP64 kinetic
+    energy sum(rho |u|^2 / 2) over all nodes and the velocity on every `sub`-th node in each
+    direction, rounded to float32 (6e-8 relative, far below the storage errors measured)."""
+    c = W.taylor_green(L=edge, u0=0.04, tau=0.51, q=27, collision=2)
+    o = oracle.OracleGrid(27, edge, edge, edge, 64)
+    o.configure(collision=2, tau=c.tau, periodic_y=1, periodic_z=1)
+    o.set_cell_types(c.types)
+    o.set_state(oracle.equilibrium(27, c.rho, c.ux, c.uy, c.uz, prec=32).astype(np.float32))
+    # initial kinetic energy from the initial fields (the equilibrium's moments reproduce them to
+    # float32 rounding); later entries from the oracle's moments after each checkpoint's step
+    ke = [0.5 * float((c.rho.astype(np.float64) * (c.ux.astype(np.float64) ** 2 + c.uy.astype(np.float64) ** 2 +
+                                                     c.uz.astype(np.float64) ** 2)).sum())]
+    u = []
+    for k in range(steps // every):
+        o.step(every)
+        m = o.macro()
+        ke.append(0.5 * float((m["rho"] * m["speed"] ** 2).sum()))
+        u.append(np.stack([m[a].reshape(edge, edge, edge)[::sub, ::sub, ::sub].astype(np.float32)
+                           for a in ("ux", "uy", "uz")]))
+        print(f"c3: step {(k + 1) * every} KE/KE0 {ke[-1] / ke[0]:.6f}", flush=True)
+    save(f"c3_tgv{edge}_mrt_fp64", edge=np.int32(edge), steps=np.int32(steps), every=np.int32(every),
+         sub=np.int32(sub), tau=np.float32(c.tau), u0=np.float32(0.04), ke=np.array(ke, np.float64),
+         u=np.stack(u))
+
+
+def diag_cases(R, steps=200):
+    """The reference's global diagnostics (compute_total_mass, compute_total_kinetic_energy,
+    compute_max_speed: serial float sums over Fluid cells only, src/grid/lattice_grid_2d.cpp:267-295,
+    src/grid/lattice_grid_3d.cpp:382-410) after `steps` steps of a cylinder channel that holds
+    Solid, Inflow and Outflow cells (TRT, the cyl2d set-up) and of a sphere with curved links
+    (TRT, the sphere3d set-up). Also stored: the same sums in FP64 over the reference's own
+    fields, over Fluid cells and over every non-solid cell."""
+    out = {}
+    c = W.cylinder_channel(nx=64, ny=32, diameter=8, cx=16, cy=16, tau=0.56, collision=1)
+    g = oracle.RefGrid2D(c.nx, c.ny, c.tau)
+    g.init_fields(c.rho, c.ux, c.uy)
+    R.ref2d_set_inflow_west(g._h, 0.05, 0.0)
+    R.ref2d_set_outflow_east(g._h, 1.0)
+    for x in range(c.nx):
+        R.ref2d_set_cell_type(g._h, x, 0, 1)
+        R.ref2d_set_cell_type(g._h, x, c.ny - 1, 1)
+    R.ref2d_set_solid_circle(g._h, 16.0, 16.0, 4.0)
+    t = g.cell_types()
+    out.update(d2_types=t, d2_f0=g.f(), d2_steps=np.int32(steps), d2_tau=np.float32(c.tau))
+    g.step(steps, 1)
+    m = g.macro()
+    out.update(d2_mass=np.float32(R.ref2d_total_mass(g._h)), d2_ke=np.float32(R.ref2d_total_ke(g._h)),
+               d2_vmax=np.float32(R.ref2d_max_speed(g._h)))
+    fluid, open_ = t == 0, t != 1
+    rho, sp = m["rho"].astype(np.float64), m["speed"].astype(np.float64)
+    out.update(d2_mass64=rho[fluid].sum(), d2_ke64=(0.5 * rho * sp * sp)[fluid].sum(),
+               d2_mass64_open=rho[open_].sum(), d2_ke64_open=(0.5 * rho * sp * sp)[open_].sum())
+    nx, ny, nz = 24, 16, 16
+    g3 = oracle.RefGrid3D(nx, ny, nz, 0.56)
+    n = nx * ny * nz
+    noise = W.uniform24(W.BASE_SEED + 600, 3 * n).reshape(3, n)
+    g3.init_fields(np.ones(n, np.float32), (0.04 + 0.01 * (noise[0] - 0.5)).astype(np.float32),
+                   (0.01 * (noise[1] - 0.5)).astype(np.float32), (0.01 * (noise[2] - 0.5)).astype(np.float32))
+    R.ref3d_set_solid_sphere(g3._h, 8.0, 8.0, 8.0, 4.0)
+    R.ref3d_build_curved_sphere_links(g3._h, 8.0, 8.0, 8.0, 4.0)
+    t3 = g3.cell_types()
+    out.update(d3_types=t3, d3_f0_sum=np.float64(g3.f().astype(np.float64).sum()), d3_steps=np.int32(steps))
+    R.ref3d_step(g3._h, 1, 0.0, 0.0, 0.0, 0, 0.14, steps)
+    m3 = g3.macro()
+    out.update(d3_mass=np.float32(R.ref3d_total_mass(g3._h)), d3_ke=np.float32(R.ref3d_total_ke(g3._h)),
+               d3_vmax=np.float32(R.ref3d_max_speed(g3._h)))
+    fl3 = t3 == 0
+    rho3, sp3 = m3["rho"].astype(np.float64), m3["speed"].astype(np.float64)
+    out.update(d3_mass64=rho3[fl3].sum(), d3_ke64=(0.5 * rho3 * sp3 * sp3)[fl3].sum())
+    save("diag", **out)
+
+
 def kat_cases(R):
     # Strouhal FFT KAT (tests/unit/test_forces_momentum_exchange.cpp:71-91)
     t = np.arange(512, dtype=np.float32)
@@ -363,6 +442,7 @@ def main():
     tgv_case(R)
     percall_cases(R)
     kat_cases(R)
+    diag_cases(R)
     c1_case(R)
     c2_case(R)
 
@@ -372,5 +452,9 @@ if __name__ == "__main__":
         c1_case(oracle.ref())
     elif "--c2" in sys.argv:  # only the full-size C2 run (about an hour on one core)
         c2_case(oracle.ref())
+    elif "--diag" in sys.argv:  # only the diagnostics fixture
+        diag_cases(oracle.ref())
+    elif "--c3" in sys.argv:  # only the FP64 Taylor-Green run (oracle only; about 30 min on 8 threads)
+        c3_case()
     else:
         main()

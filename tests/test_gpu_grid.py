@@ -310,6 +310,114 @@ def test_diagnostics_fp64():
     assert abs(vmax - m["speed"].max()) <= 1e-7
 
 
+def test_diagnostics_match_reference(golden):
+    """Global diagnostics after 200 steps against the reference's own compute_total_mass,
+    compute_total_kinetic_energy and compute_max_speed (Fluid cells only, serial float sums;
+    src/grid/lattice_grid_2d.cpp:267-295, src/grid/lattice_grid_3d.cpp:382-410), on a cylinder
+    channel holding Solid, Inflow and Outflow cells and on a walled sphere with curved links.
+    The engine sums in FP64: it must agree with the FP64 sums of the reference's own fields to
+    the fields' parity, with the reference's float sums to their accumulation error, and be far
+    from the sum over every non-solid cell (so the Fluid-only rule is what is measured)."""
+    dg = golden("diag")
+    g = wb.LatticeGrid2D(64, 32, float(dg["d2_tau"]), les_applies=False)
+    wb.check(wb.lib.wake_grid_set_inflow_west(g.handle, 0.05, 0.0, 0.0))
+    g.set_outflow_east(1.0)
+    g.set_cell_types(dg["d2_types"])
+    g.set_populations(dg["d2_f0"])
+    assert all((dg["d2_types"] == t).any() for t in (wb.SOLID, wb.INFLOW, wb.OUTFLOW))
+    g.step(wb.TRT, n=int(dg["d2_steps"]))
+    mass, ke, vmax = g._diag()
+    g.close()
+    print(f"[diag 2d] mass {mass:.9g} ref {float(dg['d2_mass']):.9g} ref-fp64 {float(dg['d2_mass64']):.9g} | "
+          f"ke {ke:.9g} ref {float(dg['d2_ke']):.9g} | vmax {vmax:.9g} ref {float(dg['d2_vmax']):.9g}")
+    assert abs(mass - dg["d2_mass64"]) <= 1e-6 * dg["d2_mass64"]
+    assert abs(ke - dg["d2_ke64"]) <= 5e-5 * dg["d2_ke64"]
+    assert abs(mass - dg["d2_mass"]) <= 1e-5 * dg["d2_mass"] and abs(ke - dg["d2_ke"]) <= 1e-4 * dg["d2_ke"]
+    assert abs(vmax - dg["d2_vmax"]) <= 1e-5 * dg["d2_vmax"]
+    assert abs(mass - dg["d2_mass64_open"]) >= 1e-2 * mass and abs(ke - dg["d2_ke64_open"]) >= 1e-2 * ke
+
+    nx, ny, nz = 24, 16, 16
+    n = nx * ny * nz
+    noise = W.uniform24(W.BASE_SEED + 600, 3 * n).reshape(3, n)
+    g3 = wb.LatticeGrid3D(nx, ny, nz, 0.56, les_applies=False)
+    g3.initialize_fields(np.ones(n, np.float32), (0.04 + 0.01 * (noise[0] - 0.5)).astype(np.float32),
+                         (0.01 * (noise[1] - 0.5)).astype(np.float32), (0.01 * (noise[2] - 0.5)).astype(np.float32))
+    g3.set_cell_types(dg["d3_types"])
+    g3.build_curved_sphere_links(8.0, 8.0, 8.0, 4.0)
+    # the same start as the reference's (its float equilibrium of these fields)
+    assert abs(g3.f_src_data().astype(np.float64).sum() - float(dg["d3_f0_sum"])) <= 1e-12 * float(dg["d3_f0_sum"])
+    g3.step(wb.TRT, n=int(dg["d3_steps"]))
+    mass, ke, vmax = g3._diag()
+    g3.close()
+    print(f"[diag 3d] mass {mass:.9g} ref {float(dg['d3_mass']):.9g} | ke {ke:.9g} ref {float(dg['d3_ke']):.9g} | "
+          f"vmax {vmax:.9g} ref {float(dg['d3_vmax']):.9g}")
+    assert abs(mass - dg["d3_mass64"]) <= 1e-6 * dg["d3_mass64"]
+    assert abs(ke - dg["d3_ke64"]) <= 5e-5 * dg["d3_ke64"]
+    assert abs(mass - dg["d3_mass"]) <= 1e-5 * dg["d3_mass"] and abs(ke - dg["d3_ke"]) <= 1e-4 * dg["d3_ke"]
+    assert abs(vmax - dg["d3_vmax"]) <= 1e-5 * dg["d3_vmax"]
+
+
+@pytest.mark.parametrize("shape", ["circle", "circle_cut", "sphere", "sphere_cut", "ellipse", "ellipse_3d"])
+def test_device_rasterisers_match_reference_rules(shape):
+    """The circle, sphere and ellipse setters mark cells on the device. The cell types equal, cell
+    for cell, the host rules they replace (the float32 restatements in workloads, which follow
+    LatticeGrid2D::set_solid_circle, lattice_grid_2d.cpp:143-158, and
+    LatticeGrid3D::set_solid_sphere, lattice_grid_3d.cpp:160-182) and, where the reference build
+    is present, the reference's own setters; shapes cut by the lattice's edges included. A host
+    edit after a device edit, and the device edit after it, keep both copies coherent."""
+    if shape.startswith("circle"):
+        nx, ny, nz = 64, 40, 1
+        args = (20.5, 18.25, 7.3) if shape == "circle" else (2.0, 37.5, 6.0)
+    elif shape.startswith("sphere"):
+        nx, ny, nz = 40, 24, 20
+        args = (12.3, 11.7, 9.9, 5.6) if shape == "sphere" else (38.0, 1.0, 18.5, 4.5)
+    else:
+        nx, ny, nz = 72, 36, 1 if shape == "ellipse" else 6
+        args = (15.0, 18.0, 8.5, 3.2, 0.3)
+    exp = np.zeros((nz, ny, nx), np.uint8)
+    if shape.startswith("circle"):
+        g = wb.LatticeGrid2D(nx, ny, 0.6)
+        g.set_solid_circle(*args)
+        W._rasterize_circle(exp[0], *args)
+    elif shape.startswith("sphere"):
+        g = wb.LatticeGrid3D(nx, ny, nz, 0.6)
+        g.set_solid_sphere(*args)
+        W._rasterize_sphere(exp, *args)
+    else:
+        g = wb.LatticeGrid2D(nx, ny, 0.6) if nz == 1 else wb.LatticeGrid3D(nx, ny, nz, 0.6)
+        wb.check(wb.lib.wake_grid_set_solid_ellipse(g.handle, *args))
+        for z in range(nz):
+            W._rasterize_ellipse(exp[z], *args)
+    got = g.cell_type_data().reshape(nz, ny, nx)
+    assert exp.any() and np.array_equal(got, exp)
+    R = oracle.ref()
+    if R is not None and shape.startswith("circle"):
+        r = oracle.RefGrid2D(nx, ny, 0.6)
+        R.ref2d_set_solid_circle(r._h, *args)
+        assert np.array_equal(r.cell_types().reshape(ny, nx), got[0])
+    if R is not None and shape.startswith("sphere"):
+        r = oracle.RefGrid3D(nx, ny, nz, 0.6)
+        R.ref3d_set_solid_sphere(r._h, *args)
+        assert np.array_equal(r.cell_types().reshape(nz, ny, nx), got)
+    # a host edit after the device edit, then another device edit
+    wb.check(wb.lib.wake_grid_set_cell_type(g.handle, 1, 1, 0, wb.OUTFLOW))
+    exp[0, 1, 1] = wb.OUTFLOW
+    wb.check(wb.lib.wake_grid_set_solid_box(g.handle, nx - 3, 0, 0, nx - 1, 1, nz - 1))
+    exp[:, 0:2, nx - 3:] = wb.SOLID
+    if shape.startswith("circle"):
+        g.set_solid_circle(nx - 10.0, 5.0, 3.0)
+        W._rasterize_circle(exp[0], nx - 10.0, 5.0, 3.0)
+    elif shape.startswith("sphere"):
+        g.set_solid_sphere(5.0, 5.0, 5.0, 3.0)
+        W._rasterize_sphere(exp, 5.0, 5.0, 5.0, 3.0)
+    else:
+        wb.check(wb.lib.wake_grid_set_solid_ellipse(g.handle, nx - 12.0, 8.0, 5.0, 2.0, 1.0))
+        for z in range(nz):
+            W._rasterize_ellipse(exp[z], nx - 12.0, 8.0, 5.0, 2.0, 1.0)
+    assert np.array_equal(g.cell_type_data().reshape(nz, ny, nx), exp)
+    g.close()
+
+
 def test_numeric_failure_is_reported():
     """A non-finite population is reported as WAKE_ERR_NUMERIC by the status word, not a fault."""
     g = wb.LatticeGrid2D(32, 16, 0.6)
@@ -344,6 +452,59 @@ def test_staged_and_direct_kernels_agree(storage, which):
     assert np.array_equal(out[0][0], out[1][0])
     if case.mem:
         assert np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+@pytest.mark.parametrize("which", ["cyl2d", "sphere3d", "sphere3d_ragged", "tgv27", "narrow"])
+def test_row_kernel_equals_span_kernel(storage, which):
+    """The whole-row TRT kernels (variant 3: one block per row, adjacent node pairs, Zou-He from
+    the row descriptor; variant 4: the same rows staged through shared memory by bulk copies,
+    several rows in flight per CTA) and the span kernel (variant 1) run the same per-node
+    arithmetic in other thread layouts: identical populations and forces after 23 steps. Covers
+    Zou-He rows (2D column rule and 3D typed faces), rows that end in a partial 64-node chunk
+    (nx = 70, 96), a 32-thread block (nx = 40) and D3Q27. Rows whose bytes are not a whole number
+    of 16-byte units (nx = 70 in 16-bit storage) cannot take bulk copies: variant 4 falls back
+    to the span kernel there."""
+    if which == "cyl2d":
+        case = W.cylinder_channel(nx=96, ny=40, diameter=8.0, cx=24.0, cy=20.0, collision=wb.TRT)
+    elif which == "sphere3d":
+        case = W.sphere_channel(nx=48, ny=24, nz=24, radius=5.0, center=(16.0, 12.0, 12.0))
+    elif which == "sphere3d_ragged":
+        case = W.sphere_channel(nx=70, ny=20, nz=18, radius=4.0, center=(20.0, 10.0, 9.0))
+    elif which == "tgv27":
+        case = W.taylor_green(L=24, u0=0.04, tau=0.56, q=27, collision=wb.TRT)
+    else:
+        case = W.cylinder_channel(nx=40, ny=24, diameter=6.0, cx=12.0, cy=12.0, collision=wb.TRT)
+    out = []
+    esize = 4 if storage == "f32" else 2
+    for variant in (1, 3, 4):
+        g = W.build_grid(case, storage=storage)
+        wb.check(wb.lib.wake_grid_set_kernel(g.handle, variant))
+        g.step(case.collision, use_les=case.les, smag_const=case.cs_smag, n=23)
+        g.synchronize()
+        expect = 1 if (variant == 4 and (case.nx * esize) % 16) else variant
+        assert wb.lib.wake_grid_get_kernel(g.handle) == expect
+        out.append((g.f_src_data().copy(), g.force_history().copy() if case.mem else None))
+        g.close()
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0])
+        if case.mem:
+            assert np.array_equal(out[0][1], o[1])
+
+
+def test_row_kernel_falls_back_where_it_cannot_run():
+    """Odd nx (rows off the word boundary) and non-TRT models keep the span kernel."""
+    odd = W.sphere_channel(nx=47, ny=16, nz=16, radius=4.0, center=(14.0, 8.0, 8.0))
+    g = W.build_grid(odd)
+    wb.check(wb.lib.wake_grid_set_kernel(g.handle, 3))
+    g.step(odd.collision, use_les=odd.les, smag_const=odd.cs_smag, n=2)
+    assert wb.lib.wake_grid_get_kernel(g.handle) == 1
+    g.close()
+    mrt = W.taylor_green(L=16, u0=0.04, tau=0.56, q=27, collision=wb.MRT)
+    g = W.build_grid(mrt)
+    g.step(mrt.collision, n=2)
+    assert wb.lib.wake_grid_get_kernel(g.handle) == 1
+    g.close()
 
 
 def test_c1_cylinder_channel_full_length_tracks_reference(golden):
@@ -428,6 +589,43 @@ def test_c2_sphere_channel_full_size_tracks_reference(golden):
           f"u gpu-ref {e_u[0]:.2e} gpu-fp64 {e_u[1]:.2e} ref-fp64 {e_u[2]:.2e} | "
           f"rho gpu-ref {e_rho[0]:.2e} gpu-fp64 {e_rho[1]:.2e} ref-fp64 {e_rho[2]:.2e}")
     assert e_cd[0] <= FORCE_TOL
-    assert e_u[0] <= max(U_TOL, 2.0 * e_u[2]) and e_rho[0] <= max(RHO_TOL, 2.0 * e_rho[2])
+    assert e_u[0] <= U_TOL and e_rho[0] <= RHO_TOL
     for e in (e_cd, e_u, e_rho):
         assert e[1] <= 2.0 * e[2] + 1e-6
+
+
+# 16-bit storage on the full-size C2 case against FP64 (velocity relative L2 on the fixture
+# planes; C_D as the relative L2 of the drag history and as the mean of the last 500 steps).
+# FP16 carries the acceptance bounds of the storage format: velocity 1e-3, C_D 0.5%. BF16 keeps
+# 8 significant bits instead of 11, so its bounds are ten and two times wider: velocity 1e-2, C_D 1%.
+@pytest.mark.skipif(not C2_FIXTURE.exists(), reason="full-size C2 fixture not generated")
+@pytest.mark.parametrize("storage,u_tol,cd_tol", [("f16", 1e-3, 5e-3), ("bf16", 1e-2, 1e-2)])
+def test_c2_sphere_channel_full_size_16bit_storage_vs_fp64(golden, storage, u_tol, cd_tol):
+    """C2 at full size and length (the reference-expressible form of the fixture above) with the
+    populations stored as FP16 / BF16 deviations f / w - 1 and FP32 arithmetic, against the FP64
+    oracle's run of the same case: velocity on the two planes within u_tol (relative L2), drag
+    within cd_tol (whole history, relative L2, and the mean of the last 500 steps)."""
+    d = golden("c2_sphere3d_trt")
+    steps = int(d["steps"])
+    c = W.sphere_channel(reference_variant=True, collision=1, les=False)
+    g = W.build_grid(c, storage=storage)
+    g.use_graph(20)
+    g.step(c.collision, use_les=False, n=steps)
+    g.synchronize()
+    m = g.macro()
+    hist = g.force_history()
+    g.close()
+    q = 0.5 * 0.05 ** 2 * np.pi * 12.0 ** 2
+    cd = hist[:, 0] / q
+    cd64 = d["forces_fp64"][:, 0].astype(np.float64) / q
+    planes = {}
+    for k in ("ux", "uy", "uz"):
+        a = m[k].reshape(c.nz, c.ny, c.nx)
+        planes[k] = np.concatenate([a[64][::2, ::2].ravel(), a[:, 64, :][::2, ::2].ravel()])
+    p64 = {k: np.concatenate([d[f"fp64_{k}_z64"].ravel(), d[f"fp64_{k}_y64"].ravel()]) for k in planes}
+    e_u = vel_rel_l2(planes, p64, ("ux", "uy", "uz"))
+    e_cd = rel_l2(cd, cd64)
+    e_cd_mean = abs(cd[-500:].mean() - cd64[-500:].mean()) / abs(cd64[-500:].mean())
+    print(f"[C2 {storage} 2000 steps] u vs FP64 {e_u:.2e} | C_D history {e_cd:.2e}, mean of last 500 {e_cd_mean:.2e}")
+    assert e_u <= u_tol
+    assert e_cd <= cd_tol and e_cd_mean <= cd_tol

@@ -102,6 +102,7 @@ _PROTOS = {
     "wake_grid_force_count": (LL, [vp]),
     "wake_grid_step": (I, [vp, I, F, F, F]),
     "wake_grid_use_graph": (I, [vp, I]),
+    "wake_grid_prepare_steps": (I, [vp, F, F, F]),
     "wake_grid_step_count": (LL, [vp]),
     "wake_grid_synchronize": (I, [vp]),
     "wake_grid_get_populations": (I, [vp, vp]),

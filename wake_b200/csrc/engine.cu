@@ -56,6 +56,17 @@ cudaError_t launch_tiles_any(int Q, int coll, int store, bool les, const StepArg
     if (Q == 19) return launch_tiles_q19(coll, store, les, a, t, stream);
     return launch_tiles_q27(coll, store, les, a, t, stream);
 }
+cudaError_t launch_rows_any(int Q, int store, bool les, const StepArgs& a, int rows, int tpb, cudaStream_t stream) {
+    if (Q == 9) return launch_rows_q9(store, les, a, rows, tpb, stream);
+    if (Q == 19) return launch_rows_q19(store, les, a, rows, tpb, stream);
+    return launch_rows_q27(store, les, a, rows, tpb, stream);
+}
+cudaError_t launch_rows_pipe_any(int Q, int store, bool les, int cap, const StepArgs& a, const PipeArgs& p,
+                                 cudaStream_t stream) {
+    if (Q == 9) return launch_rows_pipe_q9(store, les, cap, a, p, stream);
+    if (Q == 19) return launch_rows_pipe_q19(store, les, cap, a, p, stream);
+    return launch_rows_pipe_q27(store, les, cap, a, p, stream);
+}
 cudaError_t launch_initial_any(int Q, int coll, int store, bool les, const float* f0, void* a, void* b,
                                const uint8_t* flags, const Geo& geo, const Physics& phys, const Launch& L) {
     if (Q == 9) return launch_initial_q9(coll, store, les, f0, a, b, flags, geo, phys, L);
@@ -92,6 +103,67 @@ __global__ void k_link_marks(const int* __restrict__ node, int n, uint8_t* __res
         node_start[i] = k;
         flags[i] = static_cast<uint8_t>((flags[i] | FL_BFL) & ~FL_FAST);
     }
+}
+
+// Shape rasterisers on the device: one thread per cell of the shape's bounding box marks the
+// cells whose centre (integer coordinates) lies inside. The float rules are the reference
+// setters' (LatticeGrid2D::set_solid_circle, lattice_grid_2d.cpp:143-158;
+// LatticeGrid3D::set_solid_sphere, lattice_grid_3d.cpp:160-182) and the ellipse rule of
+// wake_grid_set_solid_ellipse, with every rounding explicit so that the compiler cannot
+// contract them: kind 0 circle (dx^2 + dy^2 <= r^2, every z), 1 sphere
+// (dx^2 + dy^2 + dz^2 <= r^2), 2 rotated ellipse (u^2 / a^2 + v^2 / b^2 <= 1, every z).
+__global__ void k_rasterise(uint8_t* __restrict__ types, int nx, int ny, wk::RasterBox b, wk::RasterShape sh) {
+    const int bx = b.x1 - b.x0 + 1, by = b.y1 - b.y0 + 1, bz = b.z1 - b.z0 + 1;
+    const long long n = static_cast<long long>(bx) * by * bz;
+    for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
+         t += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int x = b.x0 + static_cast<int>(t % bx);
+        const int y = b.y0 + static_cast<int>((t / bx) % by);
+        const int z = b.z0 + static_cast<int>(t / (static_cast<long long>(bx) * by));
+        const float dx = __fsub_rn(static_cast<float>(x), sh.c[0]);
+        const float dy = __fsub_rn(static_cast<float>(y), sh.c[1]);
+        bool inside;
+        if (sh.kind == 0) {
+            inside = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) <= sh.p[0];
+        } else if (sh.kind == 1) {
+            const float dz = __fsub_rn(static_cast<float>(z), sh.c[2]);
+            inside = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)) <= sh.p[0];
+        } else {
+            const float u = __fadd_rn(__fmul_rn(dx, sh.p[0]), __fmul_rn(dy, sh.p[1]));
+            const float v = __fadd_rn(__fmul_rn(-dx, sh.p[1]), __fmul_rn(dy, sh.p[0]));
+            inside = __fadd_rn(__fmul_rn(__fmul_rn(u, u), sh.p[2]), __fmul_rn(__fmul_rn(v, v), sh.p[3])) <= 1.0f;
+        }
+        if (inside) types[(static_cast<long long>(z) * ny + y) * nx + x] = CT_SOLID;
+    }
+}
+
+// Row descriptors of the whole-row kernel (rows.cuh), one warp per row: ROW_FAST when every
+// node of the row is a pure gather and Zou-He appears only as the inlet at x = 0 and the
+// outlet at x = nx - 1 (with ROW_ZH_IN / ROW_ZH_OUT for those), 0 otherwise.
+__global__ void k_row_kind(const uint8_t* __restrict__ flags, uint8_t* __restrict__ kind, int nx, int rows) {
+    const int row = blockIdx.x * (blockDim.x >> 5) + static_cast<int>(threadIdx.x >> 5);
+    if (row >= rows) return;
+    const int lane = threadIdx.x & 31;
+    const uint8_t* f = flags + static_cast<long long>(row) * nx;
+    int ok = 1, zin = 0, zout = 0;
+    for (int x = lane; x < nx; x += 32) {
+        const uint8_t fl = f[x];
+        ok &= (fl & FL_FAST) ? 1 : 0;
+        if (fl & FL_ZH_IN) {
+            if (x == 0) zin = 1;
+            else ok = 0;
+        }
+        if (fl & FL_ZH_OUT) {
+            if (x == nx - 1) zout = 1;
+            else ok = 0;
+        }
+    }
+    ok = __all_sync(0xffffffffu, ok);
+    zin = __any_sync(0xffffffffu, zin);
+    zout = __any_sync(0xffffffffu, zout);
+    if (lane == 0)
+        kind[row] = ok ? static_cast<uint8_t>(wk::ROW_FAST | (zin ? wk::ROW_ZH_IN : 0) | (zout ? wk::ROW_ZH_OUT : 0))
+                       : static_cast<uint8_t>(0);
 }
 
 // Deterministic per-block partial sums for the diagnostics:
@@ -276,6 +348,38 @@ long long idx3(const wake_grid* g, int x, int y, int z) {
 
 int upload_links(wake_grid* g);
 
+// Bring the host copy of the cell types up to date (after device-side edits).
+int host_types(wake_grid* g) {
+    if (!g->types_dev_newer) return WAKE_OK;
+    WK_CUDA(cudaMemcpyAsync(g->types.data(), g->d_types.p, g->N, cudaMemcpyDeviceToHost, g->stream));
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    g->types_dev_newer = false;
+    return WAKE_OK;
+}
+
+// Bring the device copy up to date (after host-side edits).
+int dev_types(wake_grid* g) {
+    if (!g->types_host_newer) return WAKE_OK;
+    WK_CUDA(cudaMemcpyAsync(g->d_types.p, g->types.data(), g->N, cudaMemcpyHostToDevice, g->stream));
+    WK_CUDA(cudaStreamSynchronize(g->stream));  // the host vector may change right after
+    g->types_host_newer = false;
+    return WAKE_OK;
+}
+
+// Mark the cells of a shape solid on the device (k_rasterise); the host copy follows on demand.
+int rasterise(wake_grid* g, const wk::RasterBox& b, const wk::RasterShape& sh) {
+    if (b.x1 < b.x0 || b.y1 < b.y0 || b.z1 < b.z0) return WAKE_OK;  // the box misses the lattice
+    const int r = dev_types(g);
+    if (r) return r;
+    const long long n = static_cast<long long>(b.x1 - b.x0 + 1) * (b.y1 - b.y0 + 1) * (b.z1 - b.z0 + 1);
+    const int blocks = static_cast<int>(std::min<long long>((n + 255) / 256, 148ll * 8));
+    k_rasterise<<<blocks, 256, 0, g->stream>>>(g->d_types.as<uint8_t>(), g->nx, g->ny, b, sh);
+    WK_CUDA(cudaGetLastError());
+    g->types_dev_newer = true;
+    g->geom_dirty = true;
+    return WAKE_OK;
+}
+
 // Upload types and links, rebuild flags and momentum-exchange slots.
 int rebuild_flags(wake_grid* g) {
     if (g->links_dirty) {
@@ -283,7 +387,10 @@ int rebuild_flags(wake_grid* g) {
         if (r) return r;
         g->links_dirty = false;
     }
-    WK_CUDA(cudaMemcpyAsync(g->d_types.p, g->types.data(), g->N, cudaMemcpyHostToDevice, g->stream));
+    {
+        const int r = dev_types(g);
+        if (r) return r;
+    }
     FlagCfg cfg{};
     cfg.zh_rule = (g->Q == 9) ? 1 : 2;
     cfg.inflow = g->inflow;
@@ -418,6 +525,37 @@ int rebuild_flags(wake_grid* g) {
             g->h_tiles = std::move(tiles);
             g->h_gen4 = std::move(gen4);
             g->h_mixed = std::move(mixed_spans);
+        }
+        // whole-row kernel: one descriptor byte per row (rows.cuh), kept only where it agrees
+        // with the segment classes (ROW_FAST exactly on the rows whose segments are all pure)
+        {
+            WK_CUDA(g->d_row_kind.ensure(static_cast<std::size_t>(g->rows)));
+            const int rows_per_block = 8;
+            k_row_kind<<<(g->rows + rows_per_block - 1) / rows_per_block, 32 * rows_per_block, 0, g->stream>>>(
+                g->d_flags.as<uint8_t>(), g->d_row_kind.as<uint8_t>(), g->nx, g->rows);
+            WK_CUDA(cudaGetLastError());
+            std::vector<uint8_t> kinds(static_cast<std::size_t>(g->rows));
+            WK_CUDA(cudaMemcpyAsync(kinds.data(), g->d_row_kind.p, kinds.size(), cudaMemcpyDeviceToHost, g->stream));
+            WK_CUDA(cudaStreamSynchronize(g->stream));
+            int n_rf = 0;
+            bool agree = true;
+            for (int r = 0; r < g->rows; ++r) {
+                const bool k = (kinds[r] & wk::ROW_FAST) != 0;
+                agree = agree && (k == (row_fast[r] != 0));
+                n_rf += k ? 1 : 0;
+            }
+            g->n_row_fast = agree ? n_rf : 0;
+            g->row_fast_nodes = static_cast<long long>(g->n_row_fast) * g->nx;
+            std::vector<unsigned> list;
+            if (g->n_row_fast > 0 && g->rows < (1 << 28)) {
+                list.reserve(static_cast<std::size_t>(g->n_row_fast));
+                for (int r = 0; r < g->rows; ++r)
+                    if (kinds[r] & wk::ROW_FAST) list.push_back(static_cast<unsigned>(r) | (unsigned(kinds[r]) << 28));
+                WK_CUDA(g->d_row_list.ensure(sizeof(unsigned) * list.size()));
+                WK_CUDA(cudaMemcpyAsync(g->d_row_list.p, list.data(), sizeof(unsigned) * list.size(),
+                                        cudaMemcpyHostToDevice, g->stream));
+                WK_CUDA(cudaStreamSynchronize(g->stream));  // the host list goes out of scope
+            }
         }
         g->h_fast_rows = std::move(spans);
         g->h_gen_rows = std::move(gen);
@@ -647,9 +785,17 @@ int do_steps(wake_grid* g, int n) {
         StepArgs gen = a;
         gen.rows = g->d_gen_rows.as<unsigned>();
         gen.nrows = g->n_gen;
+        // with the whole-row kernel, the pure-gather runs of the other rows go beside the general segments
+        const bool pipe_k = g->use_pipe();
+        const bool rows_k = pipe_k || g->use_rows();
+        StepArgs part = a;
+        part.spans = g->d_mixed.as<uint4>();
+        part.nspans = rows_k ? g->n_mixed : 0;
         a.spans = g->d_fast_rows.as<uint4>();
-        a.nspans = g->n_fast;
-        const bool fork = g->n_fast > 0 && g->n_gen > 0;
+        a.nspans = rows_k ? 0 : g->n_fast;
+        a.row_kind = g->d_row_kind.as<uint8_t>();
+        const bool bulk = rows_k || g->n_fast > 0;
+        const bool fork = bulk && (g->n_gen > 0 || part.nspans > 0);
         Launch side = g->launch();
         if (fork) {
             side.stream = g->side;
@@ -657,13 +803,14 @@ int do_steps(wake_grid* g, int n) {
             WK_CUDA(cudaStreamWaitEvent(g->side, g->ev_fork, 0));
         }
         WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, gen, side, false));
+        if (part.nspans > 0) WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, part, side, true));
         if (g->mem_on) {
             // the step's force from the slots the general launch just wrote (zero if none)
             k_mem_reduce<<<1, 256, 0, side.stream>>>(a.mem.contrib, a.mem.n_nodes, a.mem.hist_step, a.mem.hist,
                                                      a.mem.hist_cap);
             WK_CUDA(cudaGetLastError());
         }
-        const bool timed = g->time_bulk && a.nspans > 0;
+        const bool timed = g->time_bulk && (rows_k || a.nspans > 0);
         if (timed) {
             while (g->t_ev.size() < g->t_used + 2) {
                 cudaEvent_t e = nullptr;
@@ -672,7 +819,14 @@ int do_steps(wake_grid* g, int n) {
             }
             WK_CUDA(cudaEventRecord(g->t_ev[g->t_used], g->stream));
         }
-        WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, a, g->launch(), true));
+        if (pipe_k) {
+            const wk::PipeArgs pa{g->d_row_list.as<unsigned>(), g->n_row_fast};
+            WK_CUDA(launch_rows_pipe_any(g->Q, g->storage, g->les != 0, g->pipe_cap(), a, pa, g->stream));
+        } else if (rows_k) {
+            WK_CUDA(launch_rows_any(g->Q, g->storage, g->les != 0, a, g->rows, g->tpb_rows(), g->stream));
+        } else {
+            WK_CUDA(launch_step_any(g->Q, g->collision, g->storage, g->les != 0, a, g->launch(), true));
+        }
         if (timed) {
             WK_CUDA(cudaEventRecord(g->t_ev[g->t_used + 1], g->stream));
             g->t_used += 2;
@@ -847,7 +1001,10 @@ int wake_grid_set_cell_type(wake_grid* g, int x, int y, int z, int type) {
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
     // out-of-range coordinates are ignored, as in LatticeGrid2D::set_cell_type (lattice_grid_2d.cpp:122-126)
     if (x < 0 || x >= g->nx || y < 0 || y >= g->ny || z < 0 || z >= g->nz) return WAKE_OK;
+    const int r = host_types(g);
+    if (r) return r;
     g->types[idx3(g, x, y, z)] = static_cast<uint8_t>(type & FL_TYPE);
+    g->types_host_newer = true;
     g->geom_dirty = true;
     return WAKE_OK;
 }
@@ -855,21 +1012,28 @@ int wake_grid_set_cell_type(wake_grid* g, int x, int y, int z, int type) {
 int wake_grid_set_cell_types(wake_grid* g, const uint8_t* types) {
     if (!valid_grid(g) || !types) return set_error(WAKE_ERR_INVALID, "null argument");
     for (long long i = 0; i < g->N; ++i) g->types[i] = types[i] & FL_TYPE;
+    g->types_dev_newer = false;  // every cell overwritten
+    g->types_host_newer = true;
     g->geom_dirty = true;
     return WAKE_OK;
 }
 
 int wake_grid_get_cell_types(wake_grid* g, uint8_t* types) {
     if (!valid_grid(g) || !types) return set_error(WAKE_ERR_INVALID, "null argument");
+    const int r = host_types(g);
+    if (r) return r;
     std::memcpy(types, g->types.data(), g->N);
     return WAKE_OK;
 }
 
 int wake_grid_set_solid_box(wake_grid* g, int x0, int y0, int z0, int x1, int y1, int z1) {
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    const int r = host_types(g);
+    if (r) return r;
     for (int z = std::max(0, z0); z <= std::min(g->nz - 1, z1); ++z)
         for (int y = std::max(0, y0); y <= std::min(g->ny - 1, y1); ++y)
             for (int x = std::max(0, x0); x <= std::min(g->nx - 1, x1); ++x) g->types[idx3(g, x, y, z)] = WAKE_CELL_SOLID;
+    g->types_host_newer = true;
     g->geom_dirty = true;
     return WAKE_OK;
 }
@@ -879,39 +1043,39 @@ int wake_grid_set_solid_box(wake_grid* g, int x0, int y0, int z0, int x1, int y1
 int wake_grid_set_solid_circle(wake_grid* g, float cx, float cy, float radius) {
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
     const float r_sq = radius * radius;
-    const int min_x = std::max(0, static_cast<int>(cx - radius - 1));
-    const int max_x = std::min(g->nx - 1, static_cast<int>(cx + radius + 1));
-    const int min_y = std::max(0, static_cast<int>(cy - radius - 1));
-    const int max_y = std::min(g->ny - 1, static_cast<int>(cy + radius + 1));
-    for (int z = 0; z < g->nz; ++z)
-        for (int y = min_y; y <= max_y; ++y)
-            for (int x = min_x; x <= max_x; ++x) {
-                const float dx = static_cast<float>(x) - cx, dy = static_cast<float>(y) - cy;
-                if (dx * dx + dy * dy <= r_sq) g->types[idx3(g, x, y, z)] = WAKE_CELL_SOLID;
-            }
-    g->geom_dirty = true;
-    return WAKE_OK;
+    wk::RasterBox b{};
+    b.x0 = std::max(0, static_cast<int>(cx - radius - 1));
+    b.x1 = std::min(g->nx - 1, static_cast<int>(cx + radius + 1));
+    b.y0 = std::max(0, static_cast<int>(cy - radius - 1));
+    b.y1 = std::min(g->ny - 1, static_cast<int>(cy + radius + 1));
+    b.z0 = 0;
+    b.z1 = g->nz - 1;
+    wk::RasterShape sh{};
+    sh.kind = 0;
+    sh.c[0] = cx;
+    sh.c[1] = cy;
+    sh.p[0] = r_sq;
+    return rasterise(g, b, sh);
 }
 
 // LatticeGrid3D::set_solid_sphere (lattice_grid_3d.cpp:160-182).
 int wake_grid_set_solid_sphere(wake_grid* g, float cx, float cy, float cz, float radius) {
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
     const float r_sq = radius * radius;
-    const int min_x = std::max(0, static_cast<int>(cx - radius - 1));
-    const int max_x = std::min(g->nx - 1, static_cast<int>(cx + radius + 1));
-    const int min_y = std::max(0, static_cast<int>(cy - radius - 1));
-    const int max_y = std::min(g->ny - 1, static_cast<int>(cy + radius + 1));
-    const int min_z = std::max(0, static_cast<int>(cz - radius - 1));
-    const int max_z = std::min(g->nz - 1, static_cast<int>(cz + radius + 1));
-    for (int z = min_z; z <= max_z; ++z)
-        for (int y = min_y; y <= max_y; ++y)
-            for (int x = min_x; x <= max_x; ++x) {
-                const float dx = static_cast<float>(x) - cx, dy = static_cast<float>(y) - cy,
-                            dz = static_cast<float>(z) - cz;
-                if (dx * dx + dy * dy + dz * dz <= r_sq) g->types[idx3(g, x, y, z)] = WAKE_CELL_SOLID;
-            }
-    g->geom_dirty = true;
-    return WAKE_OK;
+    wk::RasterBox b{};
+    b.x0 = std::max(0, static_cast<int>(cx - radius - 1));
+    b.x1 = std::min(g->nx - 1, static_cast<int>(cx + radius + 1));
+    b.y0 = std::max(0, static_cast<int>(cy - radius - 1));
+    b.y1 = std::min(g->ny - 1, static_cast<int>(cy + radius + 1));
+    b.z0 = std::max(0, static_cast<int>(cz - radius - 1));
+    b.z1 = std::min(g->nz - 1, static_cast<int>(cz + radius + 1));
+    wk::RasterShape sh{};
+    sh.kind = 1;
+    sh.c[0] = cx;
+    sh.c[1] = cy;
+    sh.c[2] = cz;
+    sh.p[0] = r_sq;
+    return rasterise(g, b, sh);
 }
 
 // Rotated ellipse (no reference counterpart; same cell-centre rule and float
@@ -923,21 +1087,22 @@ int wake_grid_set_solid_ellipse(wake_grid* g, float cx, float cy, float a, float
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
     if (!(a > 0.f) || !(b > 0.f)) return set_error(WAKE_ERR_INVALID, "wake_grid_set_solid_ellipse: semi-axes must be positive");
     const float r = std::max(a, b);
-    const int min_x = std::max(0, static_cast<int>(cx - r - 1));
-    const int max_x = std::min(g->nx - 1, static_cast<int>(cx + r + 1));
-    const int min_y = std::max(0, static_cast<int>(cy - r - 1));
-    const int max_y = std::min(g->ny - 1, static_cast<int>(cy + r + 1));
-    const float c = std::cos(angle), s = std::sin(angle);
-    const float inv_a2 = 1.0f / (a * a), inv_b2 = 1.0f / (b * b);
-    for (int z = 0; z < g->nz; ++z)
-        for (int y = min_y; y <= max_y; ++y)
-            for (int x = min_x; x <= max_x; ++x) {
-                const float dx = static_cast<float>(x) - cx, dy = static_cast<float>(y) - cy;
-                const float u = dx * c + dy * s, v = -dx * s + dy * c;
-                if (u * u * inv_a2 + v * v * inv_b2 <= 1.0f) g->types[idx3(g, x, y, z)] = WAKE_CELL_SOLID;
-            }
-    g->geom_dirty = true;
-    return WAKE_OK;
+    wk::RasterBox bx{};
+    bx.x0 = std::max(0, static_cast<int>(cx - r - 1));
+    bx.x1 = std::min(g->nx - 1, static_cast<int>(cx + r + 1));
+    bx.y0 = std::max(0, static_cast<int>(cy - r - 1));
+    bx.y1 = std::min(g->ny - 1, static_cast<int>(cy + r + 1));
+    bx.z0 = 0;
+    bx.z1 = g->nz - 1;
+    wk::RasterShape sh{};
+    sh.kind = 2;
+    sh.c[0] = cx;
+    sh.c[1] = cy;
+    sh.p[0] = std::cos(angle);
+    sh.p[1] = std::sin(angle);
+    sh.p[2] = 1.0f / (a * a);
+    sh.p[3] = 1.0f / (b * b);
+    return rasterise(g, bx, sh);
 }
 
 int wake_grid_enable_thermal(wake_grid* g, float tau_t, float t_ref, float beta_g, float t_south, float t_north) {
@@ -1012,8 +1177,13 @@ int wake_grid_set_inflow_west(wake_grid* g, float ux, float uy, float uz) {
     g->uin[0] = ux;
     g->uin[1] = uy;
     g->uin[2] = uz;
+    {
+        const int r = host_types(g);
+        if (r) return r;
+    }
     for (int z = 0; z < g->nz; ++z)
         for (int y = 0; y < g->ny; ++y) g->types[idx3(g, 0, y, z)] = WAKE_CELL_INFLOW;
+    g->types_host_newer = true;
     g->geom_dirty = true;
     return WAKE_OK;
 }
@@ -1023,8 +1193,13 @@ int wake_grid_set_outflow_east(wake_grid* g, float rho_out) {
     if (!(rho_out > 0.f)) return set_error(WAKE_ERR_INVALID, "rho_out must be positive");
     g->outflow = 1;
     g->rho_out = rho_out;
+    {
+        const int r = host_types(g);
+        if (r) return r;
+    }
     for (int z = 0; z < g->nz; ++z)
         for (int y = 0; y < g->ny; ++y) g->types[idx3(g, g->nx - 1, y, z)] = WAKE_CELL_OUTFLOW;
+    g->types_host_newer = true;
     g->geom_dirty = true;
     return WAKE_OK;
 }
@@ -1037,8 +1212,13 @@ int wake_grid_set_moving_wall(wake_grid* g, float uw_x, float uw_y, float uw_z) 
     g->uw[0] = uw_x;
     g->uw[1] = uw_y;
     g->uw[2] = uw_z;
+    {
+        const int r = host_types(g);
+        if (r) return r;
+    }
     for (int z = 0; z < g->nz; ++z)
         for (int x = 0; x < g->nx; ++x) g->types[idx3(g, x, g->ny - 1, z)] = WAKE_CELL_MOVING_WALL;
+    g->types_host_newer = true;
     g->geom_dirty = true;
     return WAKE_OK;
 }
@@ -1089,7 +1269,10 @@ int wake_grid_build_curved_sphere_links(wake_grid* g, float cx, float cy, float 
     DevMem d_list, d_count;
     WK_CUDA(d_list.ensure(sizeof(int2) * cap));
     WK_CUDA(d_count.ensure(sizeof(unsigned)));
-    WK_CUDA(cudaMemcpyAsync(g->d_types.p, g->types.data(), g->N, cudaMemcpyHostToDevice, g->stream));
+    {
+        const int r = dev_types(g);
+        if (r) return r;
+    }
     WK_CUDA(cudaMemsetAsync(d_count.p, 0, sizeof(unsigned), g->stream));
     const int blocks = static_cast<int>(std::min<long long>((g->N + 255) / 256, 148ll * 16));
     k_solid_neighbours<19><<<blocks, 256, 0, g->stream>>>(g->d_types.as<uint8_t>(), g->nx, g->ny, g->nz,
@@ -1107,6 +1290,8 @@ int wake_grid_build_curved_sphere_links(wake_grid* g, float cx, float cy, float 
         std::sort(cand.begin(), cand.end(), [](const int2& a, const int2& b) { return a.x < b.x; });
     } else {
         // more boundary nodes than the list holds (solid-heavy lattice): scan on the host
+        const int r = host_types(g);
+        if (r) return r;
         for (long long i = 0; i < g->N; ++i) {
             if (g->types[i] != WAKE_CELL_FLUID) continue;
             const int x = static_cast<int>(i % g->nx), y = static_cast<int>((i / g->nx) % g->ny),
@@ -1290,42 +1475,57 @@ int wake_grid_get_force_history(wake_grid* g, double* out, int max) {
     return static_cast<int>(n);
 }
 
+// Set the body force of the next steps; the buffers hold Collide(f^k) for the body force they
+// were collided with and the reference collides f^k with this step's force, so a change
+// re-collides (prepare).
+static int set_step_force(wake_grid* g, float gx, float gy, float gz) {
+    const float gnew[3] = {gx, gy, (g->D == 3) ? gz : 0.f};
+    for (int a = 0; a < 3; ++a) g->phys.g[a] = gnew[a];
+    if (gnew[0] != g->collided_g[0] || gnew[1] != g->collided_g[1] || gnew[2] != g->collided_g[2]) g->pending = true;
+    return prepare(g);
+}
+
+// (Re)capture the graph of graph_steps steps from the current buffer parity unless the
+// instantiated one already starts there. Captures only: nothing runs on the device.
+static int capture_graph(wake_grid* g) {
+    if (g->graph_ok && g->graph_cur == g->cur) return WAKE_OK;
+    if (g->graph) {
+        cudaGraphExecDestroy(g->graph);
+        g->graph = nullptr;
+    }
+    g->graph_ok = false;
+    const int cur0 = g->cur;
+    const long long k0 = g->k;
+    cudaGraph_t graph = nullptr;
+    WK_CUDA(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+    const int r = do_steps(g, g->graph_steps);
+    cudaError_t e = cudaStreamEndCapture(g->stream, &graph);
+    g->cur = cur0;
+    g->k = k0;
+    if (r) {
+        if (graph) cudaGraphDestroy(graph);
+        return r;
+    }
+    if (e != cudaSuccess) return set_error(WAKE_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&g->graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return set_error(WAKE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    g->graph_cur = cur0;
+    g->graph_ok = true;
+    return WAKE_OK;
+}
+
 int wake_grid_step(wake_grid* g, int n, float gx, float gy, float gz) {
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
     if (n < 0) return set_error(WAKE_ERR_INVALID, "negative step count");
     if (n == 0) return WAKE_OK;
-    const float gnew[3] = {gx, gy, (g->D == 3) ? gz : 0.f};
-    for (int a = 0; a < 3; ++a) g->phys.g[a] = gnew[a];
-    // the buffers hold Collide(f^k) for the body force they were collided with;
-    // the reference collides f^k with this step's force, so re-collide on a change
-    if (gnew[0] != g->collided_g[0] || gnew[1] != g->collided_g[1] || gnew[2] != g->collided_g[2]) g->pending = true;
-    int r = prepare(g);
+    int r = set_step_force(g, gx, gy, gz);
     if (r) return r;
     int done = 0;
     if (g->graph_steps > 0 && n >= g->graph_steps && !g->time_bulk) {
-        // (re)capture a graph of graph_steps launches from the current parity
         const int gs = g->graph_steps;
-        if (!g->graph_ok || g->graph_cur != g->cur) {
-            if (g->graph) {
-                cudaGraphExecDestroy(g->graph);
-                g->graph = nullptr;
-            }
-            const int cur0 = g->cur;
-            const long long k0 = g->k;
-            cudaGraph_t graph = nullptr;
-            WK_CUDA(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
-            r = do_steps(g, gs);
-            cudaError_t e = cudaStreamEndCapture(g->stream, &graph);
-            g->cur = cur0;
-            g->k = k0;
-            if (r) return r;
-            if (e != cudaSuccess) return set_error(WAKE_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-            e = cudaGraphInstantiate(&g->graph, graph, 0);
-            cudaGraphDestroy(graph);
-            if (e != cudaSuccess) return set_error(WAKE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-            g->graph_cur = cur0;
-            g->graph_ok = true;
-        }
+        r = capture_graph(g);
+        if (r) return r;
         while (n - done >= gs && g->cur == g->graph_cur) {
             WK_CUDA(cudaGraphLaunch(g->graph, g->stream));
             g->k += gs;
@@ -1335,6 +1535,16 @@ int wake_grid_step(wake_grid* g, int n, float gx, float gy, float gz) {
         }
     }
     return do_steps(g, n - done);
+}
+
+int wake_grid_prepare_steps(wake_grid* g, float gx, float gy, float gz) {
+    if (!valid_grid(g)) return WAKE_ERR_INVALID;
+    int r = set_step_force(g, gx, gy, gz);
+    if (r) return r;
+    if (g->graph_steps > 0 && !g->time_bulk) r = capture_graph(g);
+    if (r) return r;
+    WK_CUDA(cudaStreamSynchronize(g->stream));
+    return WAKE_OK;
 }
 
 int wake_grid_use_graph(wake_grid* g, int steps_per_graph) {
@@ -1612,7 +1822,7 @@ int wake_grid_get_block(wake_grid* g) { return g ? g->tpb : WAKE_ERR_INVALID; }
 
 int wake_grid_set_kernel(wake_grid* g, int variant) {
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
-    if (variant < 0 || variant > 2) return set_error(WAKE_ERR_INVALID, "wake_grid_set_kernel: variant 0, 1 or 2");
+    if (variant < 0 || variant > 4) return set_error(WAKE_ERR_INVALID, "wake_grid_set_kernel: variant 0 to 4");
     g->kernel_variant = variant;
     g->invalidate_graph();
     return WAKE_OK;
@@ -1620,7 +1830,9 @@ int wake_grid_set_kernel(wake_grid* g, int variant) {
 
 int wake_grid_get_kernel(wake_grid* g) {
     if (!valid_grid(g)) return WAKE_ERR_INVALID;
-    return g->use_tiles() ? 2 : 1;
+    const int r = prepare(g);
+    if (r) return r;
+    return g->use_tiles() ? 2 : (g->use_pipe() ? 4 : (g->use_rows() ? 3 : 1));
 }
 
 int wake_grid_launches_per_step(wake_grid* g) {
@@ -1628,6 +1840,7 @@ int wake_grid_launches_per_step(wake_grid* g) {
     const int r = prepare(g);
     if (r) return r;
     if (g->use_tiles()) return 1 + (g->mem_on ? 1 : 0);
+    if (g->use_pipe() || g->use_rows()) return 1 + (g->n_mixed > 0 ? 1 : 0) + (g->n_gen > 0 ? 1 : 0) + (g->mem_on ? 1 : 0);
     return (g->n_fast > 0 ? 1 : 0) + (g->n_gen > 0 ? 1 : 0) + (g->mem_on ? 1 : 0);
 }
 
@@ -1651,7 +1864,7 @@ int wake_grid_bulk_launch_times(wake_grid* g, double* total_ms, long long* launc
     if (total_ms) *total_ms = sum;
     if (launches) *launches = static_cast<long long>(g->t_used / 2);
     // the persistent launch also updates the general rows
-    if (nodes_per_launch) *nodes_per_launch = g->use_tiles() ? g->N : g->fast_nodes();
+    if (nodes_per_launch) *nodes_per_launch = g->use_tiles() ? g->N : (g->use_pipe() || g->use_rows() ? g->row_fast_nodes : g->fast_nodes());
     g->t_used = 0;
     return WAKE_OK;
 }

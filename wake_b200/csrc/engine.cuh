@@ -35,11 +35,24 @@ struct HostLat {
     }
 };
 
+// Bounding box (inclusive) and shape of a device rasteriser call (k_rasterise in engine.cu).
+struct RasterBox {
+    int x0, x1, y0, y1, z0, z1;
+};
+struct RasterShape {
+    int kind;     // 0 circle, 1 sphere, 2 rotated ellipse
+    float c[3];   // centre
+    float p[4];   // circle / sphere: r^2; ellipse: cos, sin, 1/a^2, 1/b^2
+};
+
 cudaError_t launch_step_any(int Q, int coll, int store, bool les, const StepArgs& a, const Launch& L, bool fast);
 cudaError_t launch_batch_any(int Q, int coll, int store, bool les, const BatchArgs& b, int tpb, cudaStream_t stream,
                              bool fast, bool idx32);
 cudaError_t launch_tiles_any(int Q, int coll, int store, bool les, const StepArgs& a, const TileArgs& t,
                              cudaStream_t stream);
+cudaError_t launch_rows_any(int Q, int store, bool les, const StepArgs& a, int rows, int tpb, cudaStream_t stream);
+cudaError_t launch_rows_pipe_any(int Q, int store, bool les, int cap, const StepArgs& a, const PipeArgs& p,
+                                 cudaStream_t stream);
 
 }  // namespace wk
 
@@ -69,7 +82,12 @@ struct wake_grid {
     float collided_g[3] = {0.f, 0.f, 0.f};  // body force the state buffers were collided with
     float last_step_g[3] = {0.f, 0.f, 0.f};  // body force of the last executed step
     DevMem d_types, d_flags, d_status, d_nodestart;
+    // Cell types live in two copies: `types` on the host (single-cell edits, face setters,
+    // reads) and d_types on the device (flag builds, link candidates, the shape rasterisers).
+    // The flags say which copy holds edits the other lacks; copies move only when needed.
     std::vector<uint8_t> types;
+    bool types_host_newer = true;
+    bool types_dev_newer = false;
     bool geom_dirty = true;
 
     int collision = WAKE_MRT, les = 0;
@@ -111,6 +129,26 @@ struct wake_grid {
     // shared memory plus the general rows, when the row shape allows it)
     int kernel_variant = 0;
     bool use_tiles() const { return kernel_variant == 2 && wk::tile_row_ok(nx, static_cast<int>(elem)); }
+    // Whole-row TRT kernel (k_step_rows, automatic or variant 3): one block per row over the
+    // rows whose every node is a pure gather (d_row_kind, ROW_* bytes); the pure-gather runs
+    // of the other rows (d_mixed) go to k_step_fast beside the general segments.
+    DevMem d_row_kind;
+    int n_row_fast = 0;           // rows marked ROW_FAST
+    long long row_fast_nodes = 0;  // nodes in them
+    bool use_rows() const {
+        return (kernel_variant == 0 || kernel_variant == 3) && collision == WAKE_TRT && nx % 2 == 0 &&
+               static_cast<long long>(Q) * pitch < (1ll << 32) && !th.on && n_row_fast > 0;
+    }
+    int tpb_rows() const { return nx <= 64 ? 32 : 64; }
+    // Pipelined whole-row kernel (k_step_rows_pipe, variant 4): the ROW_FAST rows as
+    // (row | descriptor << 28), staged through shared memory by bulk copies.
+    DevMem d_row_list;
+    int pipe_cap() const { return nx <= 256 ? 256 : 512; }
+    bool use_pipe() const {
+        return kernel_variant == 4 && collision == WAKE_TRT && nx % 2 == 0 && nx <= 512 &&
+               (static_cast<long long>(nx) * static_cast<long long>(elem)) % 16 == 0 &&
+               static_cast<long long>(Q) * pitch < (1ll << 32) && !th.on && n_row_fast > 0 && rows < (1 << 28);
+    }
     // pure-gather tiles (0, (z << 16) | y0, rows, 0) and the segments of the other rows
     // (0, segment, general-segment entry, 0)
     DevMem d_tiles, d_gen4, d_mixed;
@@ -153,7 +191,7 @@ struct wake_grid {
         if (idle) {
             DevMem* all[] = {&A, &B, &d_types, &d_flags, &d_status, &d_nodestart, &d_link_node, &d_link_q,
                              &d_link_delta, &d_link_mom, &d_counters, &d_hist, &d_warp_base, &d_contrib,
-                             &d_fast_rows, &d_gen_rows, &d_tiles, &d_gen4, &d_mixed, &m_f, &m_rho, &m_ux, &m_uy, &m_uz,
+                             &d_fast_rows, &d_gen_rows, &d_tiles, &d_gen4, &d_mixed, &d_row_kind, &d_row_list, &m_f, &m_rho, &m_ux, &m_uy, &m_uz,
                              &m_speed, &m_diag, &TA, &TB, &m_t, &m_an};
             for (DevMem* m : all) m->release();
         }

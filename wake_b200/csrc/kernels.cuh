@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include "rowpipe.cuh"
+#include "rows.cuh"
 #include "staged.cuh"
 #include "stream_collide.cuh"
 
@@ -41,6 +43,9 @@ struct FlagCfg {
     cudaError_t launch_flags_q##Q(const uint8_t* types, uint8_t* flags, const Geo& geo, const FlagCfg& cfg,      \
                                   const Launch& L);                                                              \
     cudaError_t launch_seg_class_q##Q(const uint8_t* flags, uint8_t* cls, const Geo& geo, long long nsegs,       \
+                                      cudaStream_t stream);                                                      \
+    cudaError_t launch_rows_q##Q(int store, bool les, const StepArgs& a, int rows, int tpb, cudaStream_t stream); \
+    cudaError_t launch_rows_pipe_q##Q(int store, bool les, int cap, const StepArgs& a, const PipeArgs& p,         \
                                       cudaStream_t stream);
 
 WK_DECLARE_LAUNCHERS(9)

@@ -311,6 +311,72 @@ cudaError_t WK_CAT(launch_flags_q, WK_Q)(const uint8_t* types, uint8_t* flags, c
     return cudaGetLastError();
 }
 
+// Whole-row TRT kernel (rows.cuh): one block per row of the lattice.
+cudaError_t WK_CAT(launch_rows_q, WK_Q)(int store, bool les, const StepArgs& a, int rows, int tpb,
+                                       cudaStream_t stream) {
+    if (rows <= 0) return cudaSuccess;
+    switch (store * 2 + (les ? 1 : 0)) {
+        case 0: k_step_rows<kQ, 0, false><<<rows, tpb, 0, stream>>>(a); break;
+        case 1: k_step_rows<kQ, 0, true><<<rows, tpb, 0, stream>>>(a); break;
+        case 2: k_step_rows<kQ, 1, false><<<rows, tpb, 0, stream>>>(a); break;
+        case 3: k_step_rows<kQ, 1, true><<<rows, tpb, 0, stream>>>(a); break;
+        case 4: k_step_rows<kQ, 2, false><<<rows, tpb, 0, stream>>>(a); break;
+        case 5: k_step_rows<kQ, 2, true><<<rows, tpb, 0, stream>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+namespace {  // internal linkage: every lattice's translation unit has its own pipe_one (kQ differs)
+// Pipelined whole-row TRT kernel (rowpipe.cuh): as many CTAs as fit on the device (capped by
+// the rows), dynamic shared memory opted in once per instantiation.
+template <int S, bool LES, int CAP>
+cudaError_t pipe_one(const StepArgs& a, const PipeArgs& p, cudaStream_t stream) {
+    constexpr unsigned smem = pipe_smem_bytes<kQ, S, CAP>();
+    static int slots = 0;  // resident CTAs on the device
+    if (slots == 0) {
+        cudaError_t e = cudaFuncSetAttribute(k_step_rows_pipe<kQ, S, LES, CAP>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        // the stages are the kernel's working set: all of the SM's unified memory as shared memory
+        e = cudaFuncSetAttribute(k_step_rows_pipe<kQ, S, LES, CAP>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0, sms = 0, dev = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_rows_pipe<kQ, S, LES, CAP>,
+                                                          pipe_threads<CAP>(), smem);
+        if (e != cudaSuccess) return e;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        slots = std::max(1, per_sm * sms);
+    }
+    const int blocks = std::min(p.nrows, slots);
+    if (blocks <= 0) return cudaSuccess;
+    k_step_rows_pipe<kQ, S, LES, CAP><<<blocks, pipe_threads<CAP>(), smem, stream>>>(a, p);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t WK_CAT(launch_rows_pipe_q, WK_Q)(int store, bool les, int cap, const StepArgs& a, const PipeArgs& p,
+                                            cudaStream_t stream) {
+    const int sel = (cap > 256 ? 6 : 0) + store * 2 + (les ? 1 : 0);
+    switch (sel) {
+        case 0: return pipe_one<0, false, 256>(a, p, stream);
+        case 1: return pipe_one<0, true, 256>(a, p, stream);
+        case 2: return pipe_one<1, false, 256>(a, p, stream);
+        case 3: return pipe_one<1, true, 256>(a, p, stream);
+        case 4: return pipe_one<2, false, 256>(a, p, stream);
+        case 5: return pipe_one<2, true, 256>(a, p, stream);
+        case 6: return pipe_one<0, false, 512>(a, p, stream);
+        case 7: return pipe_one<0, true, 512>(a, p, stream);
+        case 8: return pipe_one<1, false, 512>(a, p, stream);
+        case 9: return pipe_one<1, true, 512>(a, p, stream);
+        case 10: return pipe_one<2, false, 512>(a, p, stream);
+        case 11: return pipe_one<2, true, 512>(a, p, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t WK_CAT(launch_seg_class_q, WK_Q)(const uint8_t* flags, uint8_t* cls, const Geo& geo, long long nsegs,
                                             cudaStream_t stream) {
     if (nsegs <= 0) return cudaSuccess;

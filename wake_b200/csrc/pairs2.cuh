@@ -82,10 +82,11 @@ __device__ __forceinline__ void trt_pairs2(float2* f, const Physics& P, float2& 
     u[2] = mul2(forced ? fma2(hr, bc2(g[2]), jz) : jz, inv);
     const float2 u2 = fma2(u[2], u[2], fma2(u[1], u[1], mul2(u[0], u[0])));
     const float2 a0 = fma2(bc2(-1.5f), u2, bc2(1.0f));
-    // per pair: c.u, the even equilibrium factor t = a0 + 4.5 (c.u)^2 and the
-    // non-equilibrium parts nS = s - s_eq, nD = d - d_eq
+    // per pair: c.u and the non-equilibrium parts nS = s - s_eq, nD = d - d_eq, with the even
+    // equilibrium written s_eq = (9 w rho (c.u)) (c.u) + 2 w rho a0 (h-space: w = 1 and - 2)
     float2 nS[NP], nD[NP];
-    const float2 r2 = add2(r, r), rm6 = mul2(bc2(-6.0f), r);
+    const float2 rm6 = mul2(bc2(-6.0f), r);
+    const float2 e0h = fma2(add2(r, r), a0, bc2(-2.0f)), r9 = mul2(bc2(9.0f), r);  // h-space
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
         const int q = pair_q<Q>(p);
@@ -94,13 +95,14 @@ __device__ __forceinline__ void trt_pairs2(float2* f, const Physics& P, float2& 
         float2 cu = cx ? (cx > 0 ? u[0] : neg2(u[0])) : bc2(0.f);
         if (cy) cu = cx ? acc_c(cu, cy, u[1]) : (cy > 0 ? u[1] : neg2(u[1]));
         if (cz) cu = (cx || cy) ? acc_c(cu, cz, u[2]) : (cz > 0 ? u[2] : neg2(u[2]));
-        const float2 t = fma2(mul2(bc2(4.5f), cu), cu, a0);
         if constexpr (HS) {
-            nS[p] = sub2(s[p], fma2(r2, t, bc2(-2.0f)));
+            nS[p] = sub2(s[p], fma2(mul2(r9, cu), cu, e0h));
             nD[p] = fma2(rm6, cu, d[p]);
         } else {
+            // the weight-class products (2 w rho a0, 9 w rho, -6 w rho) are shared by the pairs of a class
             const float w = L::w(q);
-            nS[p] = sub2(s[p], mul2(mul2(bc2(2.0f * w), r), t));
+            const float2 e0w = mul2(mul2(bc2(2.0f * w), r), a0);
+            nS[p] = sub2(s[p], fma2(mul2(mul2(bc2(9.0f * w), r), cu), cu, e0w));
             nD[p] = fma2(mul2(bc2(-6.0f * w), r), cu, d[p]);
         }
     }
@@ -133,7 +135,7 @@ __device__ __forceinline__ void trt_pairs2(float2* f, const Physics& P, float2& 
     }
     // rest population: relaxes to w_0 rho a0 (h-space: rho a0 - 1)
     const float2 e0 = HS ? fma2(r, a0, bc2(-1.0f)) : mul2(mul2(bc2(L::w(0)), r), a0);
-    f[0] = sub2(f[0], mul2(add2(hs, hs), sub2(f[0], e0)));
+    f[0] = fma2(mul2(bc2(-2.0f), hs), sub2(f[0], e0), f[0]);
     float2 ug;
     float2 ps, pa;
     if (forced) {
@@ -144,11 +146,22 @@ __device__ __forceinline__ void trt_pairs2(float2* f, const Physics& P, float2& 
         const float2 fr = HS ? r : mul2(bc2(L::w(0)), r);
         f[0] = fma2(mul2(ps, fr), mul2(bc2(-3.0f), ug), f[0]);
     }
+    if (!forced) {
+        // f_q' = f_q - hs nS - ha nD, f_opp' = f_opp - hs nS + ha nD, two fused steps each
+        const float2 nhs = neg2(hs), nha = neg2(ha);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const int q = pair_q<Q>(p), o = L::opp(q);
+            f[q] = fma2(nhs, nS[p], fma2(nha, nD[p], f[q]));
+            f[o] = fma2(nhs, nS[p], fma2(ha, nD[p], f[o]));
+        }
+        return;
+    }
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
         const int q = pair_q<Q>(p), o = L::opp(q);
         float2 A = mul2(hs, nS[p]), B = mul2(ha, nD[p]);
-        if (forced) {
+        {
             // Guo forcing of the pair (collide_trt_t in lattice.cuh): even part
             // (1 - omega_s/2) w rho (-3 u.g + 9 (c.u)(c.g)), odd part (1 - omega_a/2) w rho 3 (c.g)
             const float cg = float(L::cx(q)) * g[0] + float(L::cy(q)) * g[1] + float(L::cz(q)) * g[2];

@@ -22,6 +22,27 @@ namespace wk {
 namespace {
 
 // ---------------------------------------------------------------- staging
+// Where a caller's pointer lives, seen from the current device.
+enum class PtrKind { Host, Here, OtherDevice };
+
+PtrKind pointer_kind(const void* p) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return PtrKind::Host;
+    }
+    if (attr.type == cudaMemoryTypeManaged) return PtrKind::Here;
+    if (attr.type != cudaMemoryTypeDevice) return PtrKind::Host;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return PtrKind::OtherDevice;
+    }
+    // device memory of another GPU: its kernels here would read peer memory (or fault
+    // without peer access), so callers get WAKE_ERR_INVALID instead
+    return attr.device == dev ? PtrKind::Here : PtrKind::OtherDevice;
+}
+
 struct Arena {
     DevMem mem;
 };
@@ -52,6 +73,9 @@ class Stager {
     // Allocate the arena and copy staged inputs. Returns 0 or an error code.
     int begin() {
         if (bad_) return set_error(WAKE_ERR_INVALID, "null pointer argument");
+        if (foreign_)
+            return set_error(WAKE_ERR_INVALID, "pointer to another GPU's memory: make that GPU current, or pass "
+                                               "memory of the current GPU");
         if (total_ > 0) {
             const cudaError_t e = t_arena.mem.ensure(total_);
             if (e != cudaSuccess) return set_error(WAKE_ERR_NOMEM, std::string("staging: ") + cudaGetErrorString(e));
@@ -79,12 +103,9 @@ class Stager {
         Item it{p, bytes, 0, in, out, false, p};
         if (!p && bytes > 0) bad_ = true;
         if (p) {
-            cudaPointerAttributes attr{};
-            const cudaError_t e = cudaPointerGetAttributes(&attr, p);
-            const bool on_device = e == cudaSuccess &&
-                                   (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged);
-            if (e != cudaSuccess) (void)cudaGetLastError();
-            if (!on_device) {
+            const PtrKind k = pointer_kind(p);
+            if (k == PtrKind::OtherDevice) foreign_ = true;
+            if (k == PtrKind::Host) {
                 it.staged = true;
                 it.offset = total_;
                 total_ += (bytes + 255) / 256 * 256;
@@ -96,6 +117,7 @@ class Stager {
     std::vector<Item> items_;
     std::size_t total_ = 0;
     bool bad_ = false;
+    bool foreign_ = false;
 };
 
 inline int blocks_for(long long n, int t = 256) { return static_cast<int>((n + t - 1) / t); }
@@ -711,14 +733,8 @@ void* g_noalloc_scratch_addr[kNoAllocMaxDevices] = {};
 
 static __device__ __align__(256) double g_noalloc_mem_partials[3 * kNoAllocMaxBlocks];
 
-static bool device_accessible(const void* p) {
-    cudaPointerAttributes attr{};
-    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
-        (void)cudaGetLastError();
-        return false;
-    }
-    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
-}
+// Device memory of the current GPU, or managed memory.
+static bool device_accessible(const void* p) { return wk::pointer_kind(p) == wk::PtrKind::Here; }
 
 extern "C" int d3q19_compute_momentum_exchange_forces_noalloc(const float f_post_collision[],
                                                                const uint8_t cell_type[], int nx, int ny, int nz,
@@ -735,8 +751,9 @@ extern "C" int d3q19_compute_momentum_exchange_forces_noalloc(const float f_post
     const void* ptrs[5] = {f_post_collision, cell_type, fx_out, fy_out, fz_out};
     for (const void* p : ptrs)
         if (!p || !device_accessible(p))
-            return set_error(WAKE_ERR_INVALID, "momentum exchange (no-alloc): every pointer must be device or "
-                                               "managed memory (host buffers would need allocated staging)");
+            return set_error(WAKE_ERR_INVALID, "momentum exchange (no-alloc): every pointer must be memory of the "
+                                               "current GPU or managed memory (host buffers would need allocated "
+                                               "staging)");
     int dev = 0;
     WK_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kNoAllocMaxDevices)

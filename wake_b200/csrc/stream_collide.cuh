@@ -284,6 +284,7 @@ struct StepArgs {
     const uint4* spans;    // pure-gather spans (member, row, x0, x1); one block per span
     int nspans;
     Thermal th;            // D2Q9 lattices only; th.on = 0 otherwise
+    const uint8_t* row_kind;  // per-row descriptor bytes of k_step_rows (rows.cuh); one block per row
 };
 
 // Work unit of the step kernels: a segment of up to SEG consecutive nodes of one

@@ -147,6 +147,13 @@ class _Grid:
     def use_graph(self, steps_per_graph: int) -> None:
         check(lib.wake_grid_use_graph(self._h, steps_per_graph))
 
+    def prepare_steps(self, collision=MRT, gx=0.0, gy=0.0, gz=0.0, use_les=False,
+                      smag_const=DEFAULT_SMAGORINSKY_CONSTANT) -> None:
+        """Do the one-time work of the next step() with these arguments now (re-collision after a
+        change, graph capture); advances nothing (wake_grid_prepare_steps)."""
+        self._apply_model(collision, use_les, smag_const)
+        check(lib.wake_grid_prepare_steps(self._h, gx, gy, gz))
+
     def synchronize(self) -> None:
         check(lib.wake_grid_synchronize(self._h))
 
