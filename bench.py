@@ -135,14 +135,30 @@ def hbm_peak():
     return FALLBACK_HBM_GBS, "fallback"
 
 
+KERNEL_NAMES = {1: ("wk::k_step_fast<19, TRT, {S}, LES, IDX32>", "spans"), 3: ("wk::k_step_rows<19, {S}, LES>", "rows"),
+                4: ("wk::k_step_rows_pipe<19, {S}, LES, 256>", "pipe")}
+
+
+def bulk_kernel(g, storage):
+    """(name, key of profiles/traffic.json) of the bulk kernel a grid steps with."""
+    import wake_b200 as wb
+
+    name, tag = KERNEL_NAMES.get(wb.lib.wake_grid_get_kernel(g.handle), ("unknown", "unknown"))
+    return name.format(S=storage.upper()), f"d3q19_{storage}_{tag}"
+
+
 def traffic_per_launch(key):
+    """DRAM bytes (read + write) of one launch of a bulk kernel from the committed ncu capture
+    (profiles/traffic.json): not measured in this run; (bytes, source) or (None, None)."""
     f = ROOT / "profiles" / "traffic.json"
-    if f.exists():
-        try:
-            return json.loads(f.read_text()).get(key)
-        except Exception:
-            return None
-    return None
+    try:
+        d = json.loads(f.read_text())
+        e = d.get(key)
+        if isinstance(e, dict):
+            return e["bytes"], "ncu capture committed in profiles/traffic.json: " + d["_source"]
+    except Exception:
+        pass
+    return None, None
 
 
 class Clocks:
@@ -274,6 +290,43 @@ def bulk_kernel_time(g, case, steps):
     wb.check(wb.lib.wake_grid_time_bulk_launches(g.handle, 0))
     g.synchronize()
     return tot.value / max(1, cnt.value), nodes.value
+
+
+def storage_accuracy_c2(storage):
+    """The C2 sphere channel at full size and length (2000 steps) in the form the reference can
+    run, stored as `storage`, against the FP64 oracle's run of the same case kept in
+    tests/golden/c2_sphere3d_trt.npz: velocity relative L2 on the planes z = 64 and y = 64 (every
+    other node) and the drag coefficient (relative L2 of the history, and the relative error of the
+    mean of the last 500 steps)."""
+    import wake_b200 as wb  # noqa: F401
+    from wake_b200 import workloads as W
+
+    fx = ROOT / "tests" / "golden" / "c2_sphere3d_trt.npz"
+    if not fx.exists():
+        return None
+    d = np.load(fx)
+    steps = int(d["steps"])
+    c = W.sphere_channel(reference_variant=True, collision=1, les=False)
+    g = W.build_grid(c, storage=storage)
+    g.use_graph(20)
+    g.step(c.collision, use_les=False, n=steps)
+    g.synchronize()
+    m = g.macro()
+    hist = g.force_history()
+    g.close()
+    q = 0.5 * 0.05 ** 2 * math.pi * 12.0 ** 2
+    cd, cd64 = hist[:, 0] / q, d["forces_fp64"][:, 0].astype(np.float64) / q
+    got, ref = [], []
+    for k in ("ux", "uy", "uz"):
+        a = m[k].reshape(c.nz, c.ny, c.nx)
+        got.append(np.concatenate([a[64][::2, ::2].ravel(), a[:, 64, :][::2, ::2].ravel()]).astype(np.float64))
+        ref.append(np.concatenate([d[f"fp64_{k}_z64"].ravel(), d[f"fp64_{k}_y64"].ravel()]).astype(np.float64))
+    got, ref = np.concatenate(got), np.concatenate(ref)
+    return {"case": "C2 sphere channel 256x128x128, 2000 steps, reference form (x-periodic, y/z walls, no Zou-He, "
+                    "LES not applied), against the FP64 oracle", "storage": storage,
+            "u_rel_l2": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+            "cd_history_rel_l2": float(np.linalg.norm(cd - cd64) / np.linalg.norm(cd64)),
+            "cd_last500_rel": float(abs(cd[-500:].mean() - cd64[-500:].mean()) / abs(cd64[-500:].mean()))}
 
 
 BATCH_WORKLOAD = ("batched D2Q9 TRT(Lambda=1/4)+Smagorinsky(Cs=0.17) ellipse sweep: 512 domains, NX~U[64,512], NY=NX/2, semi-axes in [NY/16,NY/6], "
@@ -424,7 +477,8 @@ def tgv_leg(L=384, steps=5000, every=500, graph=20):
     FP64 kinetic energy, and the velocity relative L2 error of FP16/BF16 against FP32 at the same
     step. KE is also set against the linear viscous decay exp(-6 nu k^2 t) of this initial field
     (its Laplacian is -3 k^2 u); the vortex is nonlinear at Re = u0/(nu k) = 733, so that column is
-    context, not a gate. The FP64-oracle comparison runs at 32^3 in the tests."""
+    context, not a gate. The comparison with FP64 runs on the 96^3 cube of the committed FP64 oracle
+    run (tgv_vs_fp64)."""
     import torch
 
     import wake_b200 as wb
@@ -510,6 +564,7 @@ def tgv_leg(L=384, steps=5000, every=500, graph=20):
     del res, u
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
+    out["vs_fp64"] = tgv_vs_fp64()
     return out
 
 
@@ -530,6 +585,37 @@ REFERENCE_VARIANT = ("the reference's own LatticeGrid3D::step + momentum exchang
                      "tau0=0.52, BFL links, momentum exchange every step, in the form the reference can express: "
                      "x-periodic, y/z half-way walls, no Zou-He (the reference has no 3D Zou-He), Smagorinsky tau "
                      "computed but not applied (the reference discards it)")
+
+
+def tgv_vs_fp64(storages=("f32", "f16", "bf16")):
+    """The Taylor-Green case (D3Q27 MRT, u0 = 0.04, tau = 0.51) on the 96^3 cube of the committed FP64
+    oracle run (tests/golden/c3_tgv96_mrt_fp64.npz), per storage: every 500 steps the velocity
+    relative L2 error against FP64 (every third node in each direction) and the kinetic energy's
+    relative error."""
+    import wake_b200 as wb  # noqa: F401
+    from wake_b200 import workloads as W
+
+    fx = ROOT / "tests" / "golden" / "c3_tgv96_mrt_fp64.npz"
+    if not fx.exists():
+        return None
+    d = np.load(fx)
+    L, every, sub = int(d["edge"]), int(d["every"]), int(d["sub"])
+    case = W.taylor_green(L=L, u0=0.04, tau=0.51, q=27, collision=2)
+    out = {"case": f"D3Q27 MRT Taylor-Green {L}^3, u0=0.04, tau=0.51, {int(d['steps'])} steps, against the FP64 oracle"}
+    for st in storages:
+        g = W.build_grid(case, storage=st)
+        rows = []
+        for k in range(int(d["steps"]) // every):
+            g.step(2, n=every)
+            g.synchronize()
+            m = g.macro()
+            u = np.stack([m[a].reshape(L, L, L)[::sub, ::sub, ::sub] for a in ("ux", "uy", "uz")]).astype(np.float64)
+            ref = d["u"][k].astype(np.float64)
+            rows.append({"step": every * (k + 1), "u_rel_l2": float(np.linalg.norm(u - ref) / np.linalg.norm(ref)),
+                         "ke_rel": float(g.compute_total_kinetic_energy() / float(d["ke"][k + 1]) - 1.0)})
+        g.close()
+        out[st] = rows
+    return out
 
 
 def reference_sample(case_ref, steps, warmup, budget_s, threads=1):
@@ -668,9 +754,11 @@ def main():
     bpn = BYTES_PER_NODE[("d3q19", "f32")]
     k_ms, k_nodes = bulk_kernel_time(g, case, KERNEL_TIMING_STEPS)
     achieved = bpn * k_nodes / (k_ms * 1e-3) / 1e9
+    kname, kkey = bulk_kernel(g, "f32")
+    traffic, traffic_src = traffic_per_launch(kkey)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_source": f"{peak_kind} HBM copy bandwidth", "traffic": traffic_per_launch("d3q19_f32_bulk"),
-            "bytes_per_node": bpn, "kernel": "wk::k_step_fast<19, TRT, F32, LES, IDX32>",
+            "peak_source": f"{peak_kind} HBM copy bandwidth", "traffic": traffic, "traffic_source": traffic_src,
+            "bytes_per_node": bpn, "kernel": kname,
             "launch_ms": k_ms, "nodes_per_launch": k_nodes,
             "timing": f"CUDA events around each bulk launch over {KERNEL_TIMING_STEPS} plain steps after the timed "
                       "region; achieved = bytes_per_node x nodes_per_launch / launch_ms",
@@ -689,12 +777,17 @@ def main():
         bpn16 = BYTES_PER_NODE[("d3q19", "f16")]
         k16_ms, k16_nodes = bulk_kernel_time(g16, case, KERNEL_TIMING_STEPS)
         ach16 = bpn16 * k16_nodes / (k16_ms * 1e-3) / 1e9
+        kname16, kkey16 = bulk_kernel(g16, "f16")
+        traffic16, _ = traffic_per_launch(kkey16)
         fp16 = {"value": world * n_nodes * args.steps / (ms16 * 1e-3) / 1e6, "unit": "MLUPS",
                 "ms_per_step": ms16 / args.steps, "speedup_vs_f32": ms / ms16,
                 "roofline": {"achieved": ach16, "peak": peak, "frac": ach16 / peak, "bytes_per_node": bpn16,
-                             "launch_ms": k16_ms, "traffic": traffic_per_launch("d3q19_f16_bulk")}}
+                             "launch_ms": k16_ms, "kernel": kname16, "traffic": traffic16,
+                             "traffic_source": "as roofline.traffic_source" if traffic16 else None}}
         del g16
         torch.cuda.empty_cache()
+        fp16["accuracy_vs_fp64"] = storage_accuracy_c2("f16")
+        fp16["bf16_accuracy_vs_fp64"] = storage_accuracy_c2("bf16")
 
     # ---- end to end through the public API with host buffers
     e2e = None

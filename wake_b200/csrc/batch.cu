@@ -430,6 +430,8 @@ int wake_batch_step(wake_batch* b, int n) {
                 b->graph = nullptr;
                 return set_error(WAKE_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(e2));
             }
+            const cudaError_t e3 = cudaGraphUpload(b->graph, b->stream);
+            if (e3 != cudaSuccess) return set_error(WAKE_ERR_CUDA, std::string("batch graph upload: ") + cudaGetErrorString(e3));
             b->graph_shape = b->shape;
             b->graph_parity = p0;
         }

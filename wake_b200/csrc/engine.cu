@@ -1510,6 +1510,9 @@ static int capture_graph(wake_grid* g) {
     e = cudaGraphInstantiate(&g->graph, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return set_error(WAKE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    // move the graph's work descriptors to the device now rather than at its first launch
+    e = cudaGraphUpload(g->graph, g->stream);
+    if (e != cudaSuccess) return set_error(WAKE_ERR_CUDA, std::string("graph upload: ") + cudaGetErrorString(e));
     g->graph_cur = cur0;
     g->graph_ok = true;
     return WAKE_OK;

@@ -136,16 +136,19 @@ struct wake_grid {
     int n_row_fast = 0;           // rows marked ROW_FAST
     long long row_fast_nodes = 0;  // nodes in them
     bool use_rows() const {
-        return (kernel_variant == 0 || kernel_variant == 3) && collision == WAKE_TRT && nx % 2 == 0 &&
+        return (kernel_variant == 0 || kernel_variant == 3) && !use_pipe() && collision == WAKE_TRT && nx % 2 == 0 &&
                static_cast<long long>(Q) * pitch < (1ll << 32) && !th.on && n_row_fast > 0;
     }
     int tpb_rows() const { return nx <= 64 ? 32 : 64; }
-    // Pipelined whole-row kernel (k_step_rows_pipe, variant 4): the ROW_FAST rows as
-    // (row | descriptor << 28), staged through shared memory by bulk copies.
+    // Pipelined whole-row kernel (k_step_rows_pipe, variant 4, and the automatic choice for
+    // 16-bit storage): the ROW_FAST rows as (row | descriptor << 28), staged through shared
+    // memory by bulk copies. FP32 rows take the direct row kernel automatically (measured
+    // faster there: three CTAs per SM fill the shared memory).
     DevMem d_row_list;
     int pipe_cap() const { return nx <= 256 ? 256 : 512; }
     bool use_pipe() const {
-        return kernel_variant == 4 && collision == WAKE_TRT && nx % 2 == 0 && nx <= 512 &&
+        const bool chosen = kernel_variant == 4 || (kernel_variant == 0 && storage != 0);
+        return chosen && collision == WAKE_TRT && nx % 2 == 0 && nx <= 512 &&
                (static_cast<long long>(nx) * static_cast<long long>(elem)) % 16 == 0 &&
                static_cast<long long>(Q) * pitch < (1ll << 32) && !th.on && n_row_fast > 0 && rows < (1 << 28);
     }
