@@ -430,7 +430,79 @@ SERVE_WORKLOAD = ("served mix: Poisson arrivals of D2Q9 channel jobs (ellipse sw
                   "200-20000), admission by an HBM budget of 80% of free device memory")
 
 
-def serving_leg(rate, n_jobs, storage="f32", baseline=True, graph_steps=0, d3q19_frac=0.5):
+def serving_rates(storage="f32", steps=200, edges=(48, 64, 80, 96, 112, 128, 144, 160)):
+    """Device rates (MLUPS, CUDA events over `steps` plain steps after 20) of the served job kinds:
+    a sphere job of edge n alone through its own grid and as a batch of k equal jobs (k n^3 about
+    4.2 M nodes); 64 channel jobs of the sweep batched; 16 Rayleigh-Benard cells batched."""
+    import torch
+
+    from wake_b200 import serve as S
+    from wake_b200 import workloads as W
+    from wake_b200.batch import Batch
+
+    stream = torch.cuda.Stream()
+
+    def timed(step):
+        step(20)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step(steps)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) * 1e-3
+
+    def batched(cases):
+        b = Batch(cases[0].q, storage)
+        b.set_stream(stream.cuda_stream)
+        grids = []
+        for c in cases:
+            g = W.build_grid(c, storage=storage)
+            b.add(g, c.collision, use_les=c.les, smag_const=c.cs_smag)
+            grids.append(g)
+        sec = timed(b.step)
+        b.close()
+        for g in grids:
+            g.close()
+        return sum(c.n for c in cases) * steps / sec / 1e6
+
+    out = {"sphere": {}}
+    for n in edges:
+        c = S.sphere_job_case(n)
+        g = W.build_grid(c, storage=storage)
+        g.set_stream(stream.cuda_stream)
+        sec = timed(lambda k: g.step(c.collision, use_les=c.les, smag_const=c.cs_smag, n=k))
+        g.close()
+        k = max(1, int(round(4.2e6 / n ** 3)))
+        out["sphere"][n] = {"alone": n ** 3 * steps / sec / 1e6, "batched": batched([c] * k), "batch_members": k}
+    out["d2q9_batched"] = batched(W.ellipse_sweep(64))
+    out["thermal_batched"] = batched([S.thermal_job_case(128 + 16 * i, 1e4 * 10 ** (i % 3), W.BASE_SEED + i)
+                                      for i in range(16)])
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
+
+
+def serving_cap(jobs, rates):
+    """Device-time lower bound of a job list: every job at the best measured rate of its kind and size
+    (sphere edges between the measured ones take the nearer edge's rate). Returns (seconds,
+    sims/s of that bound, or of the arrival span when the arrivals take longer)."""
+    edges = sorted(rates["sphere"])
+    t = 0.0
+    for j in jobs:
+        if j.kind == "d3q19":
+            n = min(edges, key=lambda e: abs(e - j.dims[1]))
+            r = max(rates["sphere"][n]["alone"], rates["sphere"][n]["batched"])
+        elif j.kind == "thermal":
+            r = rates["thermal_batched"]
+        else:
+            r = rates["d2q9_batched"]
+        t += j.nodes * j.steps / (r * 1e6)
+    span = max(j.arrival for j in jobs) if jobs else 0.0
+    return t, len(jobs) / max(t, span, 1e-12)
+
+
+def serving_leg(rate, n_jobs, storage="f32", baseline=True, graph_steps=0, d3q19_frac=0.5, rates=None):
     """Continuous batching (wake_b200.serve.Server) against one-job-at-a-time plain launches on the same
     arrival list, both in real time. sims/s = jobs / makespan; latency = completion - arrival."""
     import torch
@@ -456,6 +528,11 @@ def serving_leg(rate, n_jobs, storage="f32", baseline=True, graph_steps=0, d3q19
     rep = S.Server(budget, storage=storage, max_tick_steps=100, graph_steps=graph_steps).run(jobs, realtime=True)
     out = {"rate_jobs_per_s": rate, "storage": storage, "graph_steps": graph_steps, **whole(rep)}
     out["mlups"] = out["node_steps"] / max(out["makespan_s"], 1e-9) / 1e6
+    if rates is not None and ranks.world == 1:
+        t_cap, cap = serving_cap(jobs, rates)
+        out["cap"] = {"device_seconds": t_cap, "sims_per_s": cap, "fraction": out["sims_per_s"] / cap,
+                      "rule": "every job at the best measured rate of its kind and size (serving_rates), "
+                              "or the arrival span when longer"}
     if baseline:
         torch.cuda.empty_cache()
         ranks.barrier()
@@ -708,11 +785,14 @@ def main():
         run_profile(args)
         return
     if args.serve_sweep:
+        rates = serving_rates()
+        print(json.dumps({"serving_rates_mlups": rates}), flush=True)
         for rate in [float(r) for r in args.serve_sweep.split(",")]:
             wl = SERVE_WORKLOAD if args.serve_d3q19_frac == 0.5 else \
                 SERVE_WORKLOAD.replace("50/50", f"D3Q19 fraction {args.serve_d3q19_frac}")
             print(json.dumps({"workload": wl, **serving_leg(rate, args.serve_jobs, graph_steps=args.serve_graph,
-                                                            d3q19_frac=args.serve_d3q19_frac)}), flush=True)
+                                                            d3q19_frac=args.serve_d3q19_frac, rates=rates)}),
+                  flush=True)
         return
     if args.tgv_only:
         print(json.dumps(tgv_leg(L=args.tgv_size, steps=args.tgv_steps)))
@@ -828,8 +908,11 @@ def main():
         tgv = tgv_leg(L=args.tgv_size, steps=args.tgv_steps)
     served = None
     if not args.no_serve:
+        rates = serving_rates() if world == 1 else None
         served = {"workload": SERVE_WORKLOAD, **serving_leg(args.serve_rate, args.serve_jobs,
-                                                            graph_steps=args.serve_graph)}
+                                                            graph_steps=args.serve_graph, rates=rates)}
+        if rates is not None:
+            served["device_rates_mlups"] = rates
     clocks.stop()
 
     # ---- CPU baseline (rank 0, N = 1)

@@ -22,6 +22,12 @@
 #ifndef WK_FAST_OTHER_MIN_BLOCKS
 #define WK_FAST_OTHER_MIN_BLOCKS 8
 #endif
+// D2Q9 TRT carries nine populations per node, half of D3Q19's: at 16 blocks per SM it fits 64
+// registers without spills, twice the resident warps, which its fewer loads per thread need to
+// keep enough bytes in flight.
+#ifndef WK_FAST_TRT9_MIN_BLOCKS
+#define WK_FAST_TRT9_MIN_BLOCKS 16
+#endif
 
 namespace wk {
 

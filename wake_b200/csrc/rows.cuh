@@ -50,7 +50,8 @@ __device__ __forceinline__ void store_adjacent(typename Codec<S>::T* p, float2 v
 }
 
 template <int Q, int S, bool LES>
-__global__ void __launch_bounds__(WK_FAST_MAX_THREADS, WK_FAST_TRT_MIN_BLOCKS) k_step_rows(const StepArgs a) {
+__global__ void __launch_bounds__(WK_FAST_MAX_THREADS, Q == 9 ? WK_FAST_TRT9_MIN_BLOCKS : WK_FAST_TRT_MIN_BLOCKS)
+    k_step_rows(const StepArgs a) {
     using L = Lat<Q>;
     using T = typename Codec<S>::T;
     constexpr bool HS = S != STORE_F32;

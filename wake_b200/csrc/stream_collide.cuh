@@ -665,8 +665,9 @@ __global__ void __launch_bounds__(64) k_step(const StepArgs a) {
 // TRT segments carry two nodes per thread (twice the registers, half the threads per node).
 // Register budget: WK_FAST_MAX_THREADS / WK_FAST_*_MIN_BLOCKS (common.cuh).
 template <int Q, int COLL, int S, bool LES, bool IDX32>
-__global__ void __launch_bounds__(WK_FAST_MAX_THREADS,
-                                  COLL == COLL_TRT ? WK_FAST_TRT_MIN_BLOCKS : WK_FAST_OTHER_MIN_BLOCKS)
+__global__ void __launch_bounds__(WK_FAST_MAX_THREADS, COLL == COLL_TRT ? (Q == 9 ? WK_FAST_TRT9_MIN_BLOCKS
+                                                                                   : WK_FAST_TRT_MIN_BLOCKS)
+                                                                        : WK_FAST_OTHER_MIN_BLOCKS)
     k_step_fast(const StepArgs a) {
     step_span_fast<Q, COLL, S, LES, IDX32>(a, span_decode(a.spans[blockIdx.x], a.geo));
 }
@@ -712,8 +713,9 @@ __global__ void __launch_bounds__(64) k_step_batch(const BatchArgs b) {
 }
 
 template <int Q, int COLL, int S, bool LES, bool IDX32>
-__global__ void __launch_bounds__(WK_FAST_MAX_THREADS,
-                                  COLL == COLL_TRT ? WK_FAST_TRT_MIN_BLOCKS : WK_FAST_OTHER_MIN_BLOCKS)
+__global__ void __launch_bounds__(WK_FAST_MAX_THREADS, COLL == COLL_TRT ? (Q == 9 ? WK_FAST_TRT9_MIN_BLOCKS
+                                                                                   : WK_FAST_TRT_MIN_BLOCKS)
+                                                                        : WK_FAST_OTHER_MIN_BLOCKS)
     k_step_fast_batch(const BatchArgs b) {
     const uint4 sp = b.spans[blockIdx.x];
     const StepArgs a = batch_member(b, sp.x);

@@ -107,7 +107,8 @@ def sphere_job_case(n: int, storage_les: bool = True) -> W.Case:
     """D3Q19 sphere channel of n^3 nodes: sphere radius 3n/32 at (n/4, n/2, n/2), the proportions of the
     256x128x128 sphere channel (radius 12 at x = 64 of 256, height 128)."""
     r = 3.0 * n / 32.0
-    return W.sphere_channel(nx=n, ny=n, nz=n, radius=r, center=(n / 4.0, n / 2.0, n / 2.0), les=storage_les)
+    return W.sphere_channel(nx=n, ny=n, nz=n, radius=r, center=(n / 4.0, n / 2.0, n / 2.0), les=storage_les,
+                            device_geometry=True)
 
 
 def thermal_job_case(nx: int, rayleigh: float, seed: int) -> W.Case:
@@ -150,8 +151,52 @@ def job_bytes(job: Job, storage: str) -> int:
     return int(lib.wake_grid_estimate_bytes(q, nx, ny, nz, STORAGE[storage], flags))
 
 
+# Sphere jobs at least this wide step alone through the single-lattice kernels (with CUDA graphs
+# of SOLO_GRAPH_STEPS steps): measured on one B200 (FP32, TRT + LES), n = 112..160 run at 24-29k
+# MLUPS alone, within 10% of a batch of equal jobs or faster, while smaller jobs gain 1.3-2.3x from
+# batching (device rates measured by bench.py serving_rates). Solo jobs keep the batch's row lists
+# short, and those lists are rebuilt whenever the batch's membership changes.
+SOLO_MIN_EDGE = 112
+SOLO_GRAPH_STEPS = 20
+
+
 def _class_key(job: Job):
+    if job.kind == "d3q19" and job.dims[1] >= SOLO_MIN_EDGE:
+        return ("solo", job.id)
     return (job.dims[0],) + tuple(job.model)
+
+
+class _Solo:
+    """A job large enough to fill the device by itself, stepped through its own grid on its own
+    stream (the batch interface the serving loop uses)."""
+
+    def __init__(self):
+        self.g = None
+        self.case = None
+
+    def set_stream(self, stream) -> None:
+        self.stream = stream
+
+    def use_graph(self, steps: int) -> None:
+        self.graph = steps
+
+    def add(self, g, collision, use_les=False, smag_const=0.14) -> None:
+        self.g, self.model = g, (collision, use_les, smag_const)
+        g.set_stream(self.stream)
+        g.use_graph(SOLO_GRAPH_STEPS)
+
+    def step(self, n: int) -> None:
+        c, les, cs = self.model
+        self.g.step(c, use_les=les, smag_const=cs, n=n)
+
+    def remove(self, g) -> None:
+        self.g = None
+
+    def host_seconds(self) -> dict:
+        return {}
+
+    def close(self) -> None:
+        self.g = None
 
 
 def _start(job: Job, storage: str):
@@ -267,12 +312,14 @@ class Server:
                         results.append(_finish(job, g, job.arrival, adm, t_now))
                         batches[key][0].remove(g)
                         g.close()
+                        if key[0] == "solo":
+                            batches.pop(key)[0].close()
                     used -= need
                     del resident[jid]
             for job, g, case, need, adm in staged:
                 key = _class_key(job)
                 if key not in batches:
-                    b = Batch(job.dims[0], self.storage)
+                    b = _Solo() if key[0] == "solo" else Batch(job.dims[0], self.storage)
                     st = torch.cuda.Stream()
                     b.set_stream(st.cuda_stream)
                     b.use_graph(self.graph_steps)

@@ -59,7 +59,7 @@ class Case:
     nx: int
     ny: int
     nz: int
-    types: np.ndarray          # uint8 [N]
+    types: np.ndarray | None   # uint8 [N]; None: geometry set on the device (extra["device_sphere"])
     init: tuple
     tau: float
     collision: int
@@ -270,26 +270,35 @@ def rayleigh_benard(nx: int = 128, ny: int = 64, rayleigh: float = 1e4, prandtl:
 
 
 def sphere_channel(nx=256, ny=128, nz=128, radius=12.0, center=(64.0, 64.0, 64.0), u_in=0.05, tau=0.52,
-                   collision=1, les=True, cs_smag=0.17, reference_variant=False) -> Case:
+                   collision=1, les=True, cs_smag=0.17, reference_variant=False, device_geometry=False) -> Case:
     """3D sphere in a channel.
 
     Default: Zou-He inlet u_in on x=0, outlet rho=1 on x=nx-1, periodic y/z,
     TRT + Smagorinsky. ``reference_variant`` gives the form the reference can
     express: x-periodic, y/z half-way walls, no Zou-He, LES not applied.
+    ``device_geometry`` leaves the cell types off the host: build_grid types the
+    faces and rasterises the sphere on the device (wake_grid_set_solid_sphere),
+    which gives the same cells while the sphere stays clear of the faces.
     """
-    t = np.zeros((nz, ny, nx), np.uint8)
     cx, cy, cz = center
-    _rasterize_sphere(t, cx, cy, cz, radius)
     inflow = outflow = None
     if not reference_variant:
-        t[:, :, 0] = np.where(t[:, :, 0] == SOLID, SOLID, INFLOW)
-        t[:, :, nx - 1] = np.where(t[:, :, nx - 1] == SOLID, SOLID, OUTFLOW)
         inflow, outflow = (u_in, 0.0, 0.0), 1.0
-    return Case(q=19, nx=nx, ny=ny, nz=nz, types=t.ravel(), init=("uniform", 1.0, (u_in, 0.0, 0.0)), tau=tau,
+    types, extra = None, {}
+    if device_geometry and (reference_variant or cx - radius - 1.0 > 0.0 and cx + radius + 1.0 < nx - 1):
+        extra["device_sphere"] = (cx, cy, cz, radius)
+    else:
+        t = np.zeros((nz, ny, nx), np.uint8)
+        _rasterize_sphere(t, cx, cy, cz, radius)
+        if not reference_variant:
+            t[:, :, 0] = np.where(t[:, :, 0] == SOLID, SOLID, INFLOW)
+            t[:, :, nx - 1] = np.where(t[:, :, nx - 1] == SOLID, SOLID, OUTFLOW)
+        types = t.ravel()
+    return Case(q=19, nx=nx, ny=ny, nz=nz, types=types, init=("uniform", 1.0, (u_in, 0.0, 0.0)), tau=tau,
                 collision=collision, les=les and not reference_variant, cs_smag=cs_smag, inflow=inflow,
                 outflow=outflow, periodic_y=not reference_variant, periodic_z=not reference_variant,
                 sphere=(cx, cy, cz, radius), mem=(cx, cy, cz, 2.0 * radius), ref_area=math.pi * radius * radius,
-                u_ref=u_in)
+                u_ref=u_in, extra=extra)
 
 
 def _rasterize_sphere(t: np.ndarray, cx, cy, cz, radius) -> None:
@@ -362,15 +371,21 @@ def build_grid(case: Case, storage: str = "f32", les_applies: bool = True):
         wb.check(wb.lib.wake_grid_initialize_noise(g.handle, rho0, *u0, amp, seed, off))
     else:
         g.initialize_fields(case.rho, case.ux, case.uy, case.uz if case.q != 9 else None)
-    g.set_cell_types(case.types)
+    host_types = case.types is not None
+    if host_types:
+        g.set_cell_types(case.types)
     if case.q != 9 and (case.periodic_y or case.periodic_z):
         g.set_periodic_axes(case.periodic_y, case.periodic_z)
     if case.inflow is not None:
         wb.check(wb.lib.wake_grid_set_inflow_west(g.handle, *case.inflow))
-        g.set_cell_types(case.types)  # keep the case's exact typing of the faces
+        if host_types:
+            g.set_cell_types(case.types)  # keep the case's exact typing of the faces
     if case.outflow is not None:
         g.set_outflow_east(case.outflow)
-        g.set_cell_types(case.types)
+        if host_types:
+            g.set_cell_types(case.types)
+    if case.extra.get("device_sphere") is not None:
+        g.set_solid_sphere(*case.extra["device_sphere"])
     if case.sphere is not None and case.q == 19:
         g.build_curved_sphere_links(*case.sphere)
     if case.mem is not None:
