@@ -33,7 +33,6 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-BYTES_PER_NODE = {("d3q19", "f32"): 2 * 19 * 4 + 1, ("d3q19", "f16"): 2 * 19 * 2 + 1}
 FALLBACK_HBM_GBS = 6650.0
 KERNEL_TIMING_STEPS = 200
 WORKLOAD = ("D3Q19 TRT(Lambda=1/4)+Smagorinsky(Cs=0.17, applied) tau0=0.52, sphere R=12 at (64,64,64) with BFL "
@@ -58,15 +57,16 @@ def parse():
     p.add_argument("--tgv-steps", type=int, default=5000, help="steps of the Taylor-Green leg (multiple of 500)")
     p.add_argument("--tgv-only", action="store_true", help="only the Taylor-Green leg (one JSON line)")
     p.add_argument("--tgv-size", type=int, default=384, help="edge of the Taylor-Green cube (384 = the workload)")
-    p.add_argument("--serve-rate", type=float, default=20.0, help="arrival rate of the served-mix leg (jobs/s)")
-    p.add_argument("--serve-jobs", type=int, default=60, help="jobs in the served-mix leg")
+    p.add_argument("--serve-rate", type=float, default=200.0, help="arrival rate of the served-mix leg (jobs/s)")
+    p.add_argument("--serve-jobs", type=int, default=1000,
+                   help="jobs in the served-mix leg (latency percentiles over all of them)")
     p.add_argument("--serve-d3q19-frac", type=float, default=0.5,
                    help="with --serve-sweep: share of D3Q19 sphere jobs in the mix (0.5 = the workload)")
     p.add_argument("--serve-graph", type=int, default=0, help="steps per CUDA graph inside a served batch (0: plain)")
     p.add_argument("--serve-sweep", default=None,
                    help="comma-separated arrival rates: only the served mix at each rate (one JSON line per rate)")
     p.add_argument("--graph", type=int, default=20, help="steps per captured CUDA graph (0: plain launches)")
-    p.add_argument("--profile", choices=["f32", "f16", "bf16", "vorticity"], default=None,
+    p.add_argument("--profile", choices=["f32", "f16", "bf16", "f16c", "vorticity"], default=None,
                    help="profiling mode: only warm-up + timed steps of this storage, plain launches, one JSON line "
                         "('vorticity': --steps calls of the 3D vorticity / Q-criterion kernel on 256^3 device fields)")
     p.add_argument("--block", type=int, default=0, help="threads per block of the fused step (0: automatic)")
@@ -137,6 +137,16 @@ def hbm_peak():
 
 KERNEL_NAMES = {1: ("wk::k_step_fast<19, TRT, {S}, LES, IDX32>", "spans"), 3: ("wk::k_step_rows<19, {S}, LES>", "rows"),
                 4: ("wk::k_step_rows_pipe<19, {S}, LES, 256>", "pipe")}
+
+
+def bulk_bytes_per_node(g, storage):
+    """Algorithmic DRAM bytes per node of the D3Q19 bulk launch: 19 populations read and 19
+    written, plus the node's flag byte for the span and tile kernels (variants 1, 2); the
+    whole-row kernels read one descriptor byte per row instead (under 0.01 B per node)."""
+    import wake_b200 as wb
+
+    flag = 1 if wb.lib.wake_grid_get_kernel(g.handle) in (1, 2) else 0
+    return 2 * 19 * (4 if storage == "f32" else 2) + flag
 
 
 def bulk_kernel(g, storage):
@@ -566,7 +576,7 @@ def tgv_leg(L=384, steps=5000, every=500, graph=20):
     fields = W.taylor_green_fields_device(L, u0)
     stream = torch.cuda.Stream()
     grids = {}
-    for st in ("f32", "f16", "bf16"):
+    for st in ("f32", "f16", "bf16", "f16c"):
         g = wb.LatticeGrid3DQ27(L, L, L, tau, storage=st)
         g.set_stream(stream.cuda_stream)
         g.initialize_fields(*fields)
@@ -614,7 +624,7 @@ def tgv_leg(L=384, steps=5000, every=500, graph=20):
         out[st] = {"mlups": mlups, "ms_per_step": ms[st] / max(1, timed_steps_done), "bytes_per_node": bpn,
                    "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peak if gbs else None}
     if out["f32"]["mlups"]:
-        for st in ("f16", "bf16"):
+        for st in ("f16", "bf16", "f16c"):
             out[st]["speedup_vs_f32"] = out[st]["mlups"] / out["f32"]["mlups"]
     for g in grids.values():
         g.close()
@@ -664,7 +674,7 @@ REFERENCE_VARIANT = ("the reference's own LatticeGrid3D::step + momentum exchang
                      "computed but not applied (the reference discards it)")
 
 
-def tgv_vs_fp64(storages=("f32", "f16", "bf16")):
+def tgv_vs_fp64(storages=("f32", "f16", "bf16", "f16c")):
     """The Taylor-Green case (D3Q27 MRT, u0 = 0.04, tau = 0.51) on the 96^3 cube of the committed FP64
     oracle run (tests/golden/c3_tgv96_mrt_fp64.npz), per storage: every 500 steps the velocity
     relative L2 error against FP64 (every third node in each direction) and the kinetic energy's
@@ -831,7 +841,7 @@ def main():
     ms_step = ms / args.steps
     value = world * n_nodes * args.steps / (ms * 1e-3) / 1e6
     launches_per_step = wb.check(wb.lib.wake_grid_launches_per_step(g.handle))
-    bpn = BYTES_PER_NODE[("d3q19", "f32")]
+    bpn = bulk_bytes_per_node(g, "f32")
     k_ms, k_nodes = bulk_kernel_time(g, case, KERNEL_TIMING_STEPS)
     achieved = bpn * k_nodes / (k_ms * 1e-3) / 1e9
     kname, kkey = bulk_kernel(g, "f32")
@@ -847,27 +857,35 @@ def main():
     del g
     torch.cuda.empty_cache()
 
-    # ---- FP16-storage leg
-    fp16 = None
-    if not args.no_fp16:
-        g16 = W.build_grid(case, storage="f16")
+    # ---- 16-bit storage legs: FP16 (the addition's format) and FP16C
+    def storage_leg(st):
+        g16 = W.build_grid(case, storage=st)
         if args.graph:
             g16.use_graph(args.graph)
         ms16 = timed_steps(g16, case, args.steps, args.warmup, world)
-        bpn16 = BYTES_PER_NODE[("d3q19", "f16")]
+        bpn16 = bulk_bytes_per_node(g16, st)
         k16_ms, k16_nodes = bulk_kernel_time(g16, case, KERNEL_TIMING_STEPS)
         ach16 = bpn16 * k16_nodes / (k16_ms * 1e-3) / 1e9
-        kname16, kkey16 = bulk_kernel(g16, "f16")
+        kname16, kkey16 = bulk_kernel(g16, st)
         traffic16, _ = traffic_per_launch(kkey16)
-        fp16 = {"value": world * n_nodes * args.steps / (ms16 * 1e-3) / 1e6, "unit": "MLUPS",
-                "ms_per_step": ms16 / args.steps, "speedup_vs_f32": ms / ms16,
-                "roofline": {"achieved": ach16, "peak": peak, "frac": ach16 / peak, "bytes_per_node": bpn16,
-                             "launch_ms": k16_ms, "kernel": kname16, "traffic": traffic16,
-                             "traffic_source": "as roofline.traffic_source" if traffic16 else None}}
+        leg = {"value": world * n_nodes * args.steps / (ms16 * 1e-3) / 1e6, "unit": "MLUPS",
+               "ms_per_step": ms16 / args.steps, "speedup_vs_f32": ms / ms16,
+               "roofline": {"achieved": ach16, "peak": peak, "frac": ach16 / peak, "bytes_per_node": bpn16,
+                            "launch_ms": k16_ms, "kernel": kname16, "traffic": traffic16,
+                            "traffic_source": "as roofline.traffic_source" if traffic16 else None}}
         del g16
         torch.cuda.empty_cache()
+        return leg
+
+    fp16 = None
+    if not args.no_fp16:
+        fp16 = storage_leg("f16")
         fp16["accuracy_vs_fp64"] = storage_accuracy_c2("f16")
         fp16["bf16_accuracy_vs_fp64"] = storage_accuracy_c2("bf16")
+        fp16["f16c"] = storage_leg("f16c")
+        fp16["f16c"]["format"] = ("FP16C of h = f/w - 1: 1 sign, 4 exponent, 11 mantissa bits (Lehmann et al., "
+                                  "Phys. Rev. E 106, 015308, 2022), |h| < 2")
+        fp16["f16c"]["accuracy_vs_fp64"] = storage_accuracy_c2("f16c")
 
     # ---- end to end through the public API with host buffers
     e2e = None

@@ -186,6 +186,7 @@ typedef struct wake_grid wake_grid;
 #define WAKE_STORE_F32 0
 #define WAKE_STORE_F16 1   /* FP16 of f_q / w_q - 1 */
 #define WAKE_STORE_BF16 2  /* BF16 of f_q / w_q - 1 */
+#define WAKE_STORE_F16C 3  /* FP16C (1 sign, 4 exponent, 11 mantissa bits; |h| < 2) of h = f_q / w_q - 1 */
 
 /* Collision models (values of the reference's CollisionType, include/wake/core/types.hpp:80-85). */
 #define WAKE_BGK 0
@@ -305,13 +306,18 @@ void* wake_grid_state_buffer(wake_grid* g, int which);
 int wake_grid_set_block(wake_grid* g, int threads_per_block);
 int wake_grid_get_block(wake_grid* g);
 /* Step kernels: 0 automatic (default), 1 direct (a launch over the pure-gather
- * rows reading global memory, beside a launch over the remaining rows), 2 one
+ * spans reading global memory, beside a launch over the remaining rows), 2 one
  * persistent launch per step that stages the pure-gather rows in shared memory
  * by bulk copies, tiles of up to 1024 nodes, and runs the remaining rows beside
  * them (used when a row is a whole number of 16-byte chunks and at most 1024
- * nodes; otherwise the direct kernels run). get_kernel returns the kernels in
- * use (1 or 2). For TRT both compute two nodes per thread in packed FP32 with
- * the same roundings. No reference counterpart. */
+ * nodes), 3 (TRT) one block per row whose every node is a pure gather, 4 (TRT)
+ * those rows moved through shared memory by bulk copies in both directions, a
+ * few rows in flight per block (rows of at most 512 nodes and a whole number of
+ * 16-byte chunks). A variant whose conditions do not hold runs the direct
+ * kernels. Automatic: 4 for 16-bit storage where it applies, else 1.
+ * get_kernel prepares the grid and returns the variant in use (1 to 4). For
+ * TRT every variant computes two nodes per thread in packed FP32 with the same
+ * roundings, so all give the same bits. No reference counterpart. */
 int wake_grid_set_kernel(wake_grid* g, int variant);
 int wake_grid_get_kernel(wake_grid* g);
 /* Kernel launches one fused step issues with the current geometry (pure-gather

@@ -139,7 +139,7 @@ def test_batch_autotune_keeps_results():
     b.close()
 
 
-@pytest.mark.parametrize("storage", ["f16", "bf16"])
+@pytest.mark.parametrize("storage", ["f16", "bf16", "f16c"])
 def test_batch_shifted_storage_equals_alone(storage):
     cases = _sweep(3, seed_first=30)
     grids = [W.build_grid(c, storage=storage) for c in cases]

@@ -216,9 +216,91 @@ def test_d3q27_taylor_green_matches_oracle(collision):
     assert e64 <= max(U_TOL, 2.0 * e_o64)
 
 
-@pytest.mark.parametrize("storage,tol", [("f16", 1e-3), ("bf16", 1e-2)])
+def f16c_encode_np(h):
+    """The FP16C encoder restated in numpy (float32 arithmetic with subnormals): h 2^-112, then
+    half a unit of bit 12 added to the magnitude bits (nearest, ties away from zero), magnitudes
+    from 2 - 2^-12 up saturating at 2 - 2^-11; sign in bit 15, exponent in 11..14, mantissa below."""
+    u = (np.asarray(h, np.float32) * np.float32(2.0 ** -112)).view(np.uint32)
+    mag = np.minimum((u & np.uint32(0x7FFFFFFF)) + np.uint32(0x800), np.uint32(0x07FFFFFF))
+    return (((u >> np.uint32(16)) & np.uint32(0x8000)) | (mag >> np.uint32(12))).astype(np.uint16)
+
+
+def f16c_decode_np(b):
+    """FP16C bits to float32: (-1)^s 2^(E-15) (1 + m/2^11), subnormals 2^-14 m/2^11 for E = 0."""
+    b = np.asarray(b, np.uint32)
+    u = ((b & np.uint32(0x8000)) << np.uint32(16)) | ((b & np.uint32(0x7FFF)) << np.uint32(12))
+    return u.view(np.float32) * np.float32(2.0 ** 112)
+
+
+def _device_array(ptr, count, typestr):
+    """Copy `count` elements at a device address to a host numpy array (through torch)."""
+    import torch
+
+    class _View:
+        pass
+
+    v = _View()
+    v.__cuda_array_interface__ = {"shape": (count,), "typestr": typestr, "data": (int(ptr), False), "version": 2}
+    return torch.as_tensor(v, device="cuda").cpu().numpy()
+
+
+def test_f16c_codec_is_bit_exact():
+    """FP16C storage against the numpy restatement of the format. Solid nodes keep their initial
+    populations in both state buffers, encoded once from f / w - 1 (one float32 fma), so their raw
+    bits test the encoder: ordinary values, subnormals (|h| < 2^-14), zero, ties and saturation
+    (|h| >= 2). The populations the grid reports at those nodes, w + w h (one fma), test the
+    decoder."""
+    import ctypes
+
+    nx, ny = 64, 32
+    n = nx * ny
+    g = wb.LatticeGrid2D(nx, ny, 0.6, storage="f16c")
+    rng = np.random.default_rng(20261204)
+    types = np.where(rng.random(n) < 0.6, 1, 0).astype(np.uint8)
+    types[:6] = 1  # the special values below sit at solid nodes
+    h = np.concatenate([rng.uniform(-1.9, 1.9, 9 * n // 2), rng.uniform(-1, 1, 9 * n // 4) * 1e-5,
+                        rng.uniform(-4, 4, 9 * n // 8), np.zeros(9 * n - 9 * n // 2 - 9 * n // 4 - 9 * n // 8)])
+    h = rng.permutation(h).astype(np.float32).reshape(9, n)
+    h[:, :6] = np.array([2.0 ** -14, -(2.0 ** -14) * 0.999, 1.9995117, -2.0, 1e-30, -0.0], np.float32)
+    fluid = types == 0
+    h[:, fluid] = rng.uniform(-0.01, 0.01, (9, int(fluid.sum())))  # the fluid nodes step: a sane state
+    w = oracle.equilibrium(9, np.ones(1), np.zeros(1), np.zeros(1), None, prec=32).astype(np.float32).reshape(9, 1)
+    f0 = (w * (np.float32(1.0) + h)).astype(np.float32)
+    g.set_cell_types(types)
+    g.set_populations(f0)
+    g.step(wb.TRT, n=1)
+    g.synchronize()
+    q_, nx_, ny_, nz_, st_, pitch = (ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int(),
+                                     ctypes.c_longlong())
+    wb.check(wb.lib.wake_grid_info(g.handle, *[ctypes.byref(x) for x in (q_, nx_, ny_, nz_, st_)],
+                                   ctypes.byref(pitch)))
+    assert st_.value == 3
+    P = pitch.value
+    # what the device encodes: fmaf(f, 1/w, -1) in float32 (the exact value rounded once)
+    r = (np.float32(1.0) / w).astype(np.float32)
+    h_dev = (f0.astype(np.longdouble) * r.astype(np.longdouble) - 1).astype(np.float32)
+    solid = types == 1
+    expect = f16c_encode_np(h_dev)[:, solid]
+    for which in (0, 1):
+        raw = _device_array(wb.lib.wake_grid_state_buffer(g.handle, which), 9 * P, "<i2").view(np.uint16)
+        raw = raw.reshape(9, P)[:, :n]
+        got = raw[:, solid]
+        assert np.array_equal(got, expect), f"buffer {which}: {np.count_nonzero(got != expect)} values differ"
+    # decoder: the reported populations at solid nodes are w + w h(bits), one fma
+    dec = f16c_decode_np(expect).astype(np.longdouble)
+    f_expect = (w.astype(np.longdouble) * dec + w.astype(np.longdouble)).astype(np.float32)
+    f_got = g.f_src_data()[:, solid]
+    assert np.array_equal(f_got.view(np.uint32), f_expect.view(np.uint32))
+    # the format: saturation at 2 - 2^-11, subnormal steps of 2^-25, 12 significant bits
+    assert f16c_decode_np(f16c_encode_np([3.0]))[0] == np.float32(2.0 - 2.0 ** -11)
+    assert f16c_decode_np(f16c_encode_np([1.5 * 2.0 ** -25]))[0] == np.float32(2.0 ** -24)
+    assert f16c_decode_np(f16c_encode_np([1.0 + 2.0 ** -12]))[0] == np.float32(1.0 + 2.0 ** -11)
+    g.close()
+
+
+@pytest.mark.parametrize("storage,tol", [("f16", 1e-3), ("bf16", 1e-2), ("f16c", 1e-3)])
 def test_shifted_storage_error_vs_fp64(storage, tol):
-    """FP16 / BF16 storage of f/w - 1 with FP32 arithmetic: velocity error vs the FP64 oracle."""
+    """FP16 / BF16 / FP16C storage of f/w - 1 with FP32 arithmetic: velocity error vs the FP64 oracle."""
     case = W.taylor_green(L=32, u0=0.04, tau=0.51, q=27, collision=wb.MRT)
     steps = 100
     g = _run_case_gpu(case, steps, storage=storage)
@@ -247,16 +329,17 @@ C3_FIXTURE = Path(__file__).resolve().parent / "golden" / "c3_tgv96_mrt_fp64.npz
 @pytest.mark.skipif(not C3_FIXTURE.exists(), reason="FP64 Taylor-Green fixture not generated")
 def test_c3_taylor_green_storages_vs_fp64(golden):
     """The C3 Taylor-Green vortex (D3Q27 MRT, u0 = 0.04, tau = 0.51, 5000 steps) on a 96^3 cube
-    against the FP64 oracle's run (committed fixture), velocity relative L2 every 500 steps. At
-    this size the vortex breaks down (kinetic energy falls to 17% by step 5000), so errors grow
-    with the flow's own sensitivity. Bounds: FP32 2e-5 throughout; FP16 2e-3 up to step 1000 and
-    1e-2 to the end. BF16 (8 significant bits) is reported, not bounded: it leaves the FP64
-    solution by about 4% per 500 steps here."""
+    against the FP64 oracle's run (committed fixture), velocity relative L2 every 500 steps. FP32
+    stays within 1e-5 of FP64 to the end, so what grows in the 16-bit storages is their own
+    rounding, accumulated step after step. Bounds: FP32 2e-5 throughout; FP16 2e-3 up to step 1000
+    and 1e-2 to the end; FP16C (one more significant bit, same range for h) 1e-3 throughout. BF16
+    (8 significant bits) is reported, not bounded: it leaves the FP64 solution by about 4% per
+    500 steps here."""
     d = golden("c3_tgv96_mrt_fp64")
     L, every, sub = int(d["edge"]), int(d["every"]), int(d["sub"])
     case = W.taylor_green(L=L, u0=0.04, tau=0.51, q=27, collision=wb.MRT)
     errs = {}
-    for st in ("f32", "f16", "bf16"):
+    for st in ("f32", "f16", "bf16", "f16c"):
         g = W.build_grid(case, storage=st)
         e = []
         for k in range(int(d["steps"]) // every):
@@ -270,6 +353,7 @@ def test_c3_taylor_green_storages_vs_fp64(golden):
         print(f"[C3 96^3 {st}] velocity vs FP64 every {every} steps: " + " ".join(f"{x:.1e}" for x in e))
     assert np.all(errs["f32"] <= 2e-5)
     assert np.all(errs["f16"][:2] <= 2e-3) and np.all(errs["f16"] <= 1e-2)
+    assert np.all(errs["f16c"] <= 1e-3)
     assert np.all(np.isfinite(errs["bf16"]))
 
 
@@ -461,7 +545,7 @@ def test_numeric_failure_is_reported():
         g.synchronize()
 
 
-@pytest.mark.parametrize("storage", ["f32", "f16"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "f16c"])
 @pytest.mark.parametrize("which", ["cyl2d", "sphere3d", "tgv27"])
 def test_staged_and_direct_kernels_agree(storage, which):
     """The persistent tile kernel (pure-gather rows staged in shared memory) and the direct
@@ -486,7 +570,7 @@ def test_staged_and_direct_kernels_agree(storage, which):
         assert np.array_equal(out[0][1], out[1][1])
 
 
-@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f16c"])
 @pytest.mark.parametrize("which", ["cyl2d", "sphere3d", "sphere3d_ragged", "tgv27", "narrow"])
 def test_row_kernel_equals_span_kernel(storage, which):
     """The whole-row TRT kernels (variant 3: one block per row, adjacent node pairs, Zou-He from
@@ -628,13 +712,14 @@ def test_c2_sphere_channel_full_size_tracks_reference(golden):
 
 # 16-bit storage on the full-size C2 case against FP64 (velocity relative L2 on the fixture
 # planes; C_D as the relative L2 of the drag history and as the mean of the last 500 steps).
-# FP16 carries the acceptance bounds of the storage format: velocity 1e-3, C_D 0.5%. BF16 keeps
-# 8 significant bits instead of 11, so its bounds are ten and two times wider: velocity 1e-2, C_D 1%.
+# FP16 and FP16C (12 significant bits) carry the acceptance bounds of a 16-bit storage: velocity
+# 1e-3, C_D 0.5%. BF16 keeps 8 significant bits instead of 11, so its bounds are ten and two times
+# wider: velocity 1e-2, C_D 1%.
 @pytest.mark.skipif(not C2_FIXTURE.exists(), reason="full-size C2 fixture not generated")
-@pytest.mark.parametrize("storage,u_tol,cd_tol", [("f16", 1e-3, 5e-3), ("bf16", 1e-2, 1e-2)])
+@pytest.mark.parametrize("storage,u_tol,cd_tol", [("f16", 1e-3, 5e-3), ("bf16", 1e-2, 1e-2), ("f16c", 1e-3, 5e-3)])
 def test_c2_sphere_channel_full_size_16bit_storage_vs_fp64(golden, storage, u_tol, cd_tol):
     """C2 at full size and length (the reference-expressible form of the fixture above) with the
-    populations stored as FP16 / BF16 deviations f / w - 1 and FP32 arithmetic, against the FP64
+    populations stored as FP16 / BF16 / FP16C deviations f / w - 1 and FP32 arithmetic, against the FP64
     oracle's run of the same case: velocity on the two planes within u_tol (relative L2), drag
     within cd_tol (whole history, relative L2, and the mean of the last 500 steps)."""
     d = golden("c2_sphere3d_trt")

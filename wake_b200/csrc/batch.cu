@@ -283,7 +283,7 @@ int batch_prepare(wake_batch* b) {
 extern "C" {
 
 wake_batch* wake_batch_create(int q, int storage) {
-    if (!(q == 9 || q == 19 || q == 27) || storage < 0 || storage > 2) {
+    if (!(q == 9 || q == 19 || q == 27) || storage < 0 || storage > 3) {
         set_error(WAKE_ERR_INVALID, "wake_batch_create: invalid lattice or storage");
         return nullptr;
     }

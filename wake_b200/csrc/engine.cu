@@ -896,7 +896,7 @@ const char* wake_gpu_version(void) { return "wake_b200 0.1.0 (sm_100a)"; }
 
 wake_grid* wake_grid_create(int q, int nx, int ny, int nz, float tau, int storage) {
     if (!(q == 9 || q == 19 || q == 27) || nx < 1 || ny < 1 || nz < 1 || (q == 9 && nz != 1) ||
-        storage < 0 || storage > 2 || !(tau > 0.5f)) {
+        storage < 0 || storage > 3 || !(tau > 0.5f)) {
         set_error(WAKE_ERR_INVALID, "wake_grid_create: invalid lattice, size, tau or storage");
         return nullptr;
     }
@@ -1770,7 +1770,7 @@ long long wake_grid_device_bytes(wake_grid* g) {
 long long wake_grid_estimate_bytes(int q, int nx, int ny, int nz, int storage, int with_fields) {
     const bool thermal = (with_fields & 2) != 0;
     with_fields &= 1;
-    if (!(q == 9 || q == 19 || q == 27) || nx < 1 || ny < 1 || nz < 1 || storage < 0 || storage > 2)
+    if (!(q == 9 || q == 19 || q == 27) || nx < 1 || ny < 1 || nz < 1 || storage < 0 || storage > 3)
         return set_error(WAKE_ERR_INVALID, "wake_grid_estimate_bytes: invalid lattice, size or storage");
     const long long N = static_cast<long long>(nx) * ny * nz, pitch = (N + 63) / 64 * 64;
     const long long elem = storage == WAKE_STORE_F32 ? 4 : 2;

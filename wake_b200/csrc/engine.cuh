@@ -129,21 +129,22 @@ struct wake_grid {
     // shared memory plus the general rows, when the row shape allows it)
     int kernel_variant = 0;
     bool use_tiles() const { return kernel_variant == 2 && wk::tile_row_ok(nx, static_cast<int>(elem)); }
-    // Whole-row TRT kernel (k_step_rows, automatic or variant 3): one block per row over the
-    // rows whose every node is a pure gather (d_row_kind, ROW_* bytes); the pure-gather runs
-    // of the other rows (d_mixed) go to k_step_fast beside the general segments.
+    // Whole-row TRT kernel (k_step_rows, variant 3): one block per row over the rows whose
+    // every node is a pure gather (d_row_kind, ROW_* bytes); the pure-gather runs of the other
+    // rows (d_mixed) go to k_step_fast beside the general segments. Not automatic: on the D3Q19
+    // sphere channel the span kernel moves FP32 rows 3 % faster per node.
     DevMem d_row_kind;
     int n_row_fast = 0;           // rows marked ROW_FAST
     long long row_fast_nodes = 0;  // nodes in them
     bool use_rows() const {
-        return (kernel_variant == 0 || kernel_variant == 3) && !use_pipe() && collision == WAKE_TRT && nx % 2 == 0 &&
+        return kernel_variant == 3 && collision == WAKE_TRT && nx % 2 == 0 &&
                static_cast<long long>(Q) * pitch < (1ll << 32) && !th.on && n_row_fast > 0;
     }
     int tpb_rows() const { return nx <= 64 ? 32 : 64; }
     // Pipelined whole-row kernel (k_step_rows_pipe, variant 4, and the automatic choice for
     // 16-bit storage): the ROW_FAST rows as (row | descriptor << 28), staged through shared
-    // memory by bulk copies. FP32 rows take the direct row kernel automatically (measured
-    // faster there: three CTAs per SM fill the shared memory).
+    // memory by bulk copies. FP32 takes the span kernel automatically (measured faster there:
+    // three CTAs per SM fill the shared memory).
     DevMem d_row_list;
     int pipe_cap() const { return nx <= 256 ? 256 : 512; }
     bool use_pipe() const {

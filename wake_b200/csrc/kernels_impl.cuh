@@ -200,26 +200,26 @@ using InitFn = void (*)(const float*, void*, void*, const uint8_t*, const Geo&, 
 
 #define WK_ROW(C, S) {step_one<C, S, false>, step_one<C, S, true>}
 #define WK_IROW(C, S) {initial_one<C, S, false>, initial_one<C, S, true>}
-const StepFn kStep[3][3][2] = {{WK_ROW(0, 0), WK_ROW(0, 1), WK_ROW(0, 2)},
-                               {WK_ROW(1, 0), WK_ROW(1, 1), WK_ROW(1, 2)},
-                               {WK_ROW(2, 0), WK_ROW(2, 1), WK_ROW(2, 2)}};
-const InitFn kInit[3][3][2] = {{WK_IROW(0, 0), WK_IROW(0, 1), WK_IROW(0, 2)},
-                               {WK_IROW(1, 0), WK_IROW(1, 1), WK_IROW(1, 2)},
-                               {WK_IROW(2, 0), WK_IROW(2, 1), WK_IROW(2, 2)}};
+const StepFn kStep[3][4][2] = {{WK_ROW(0, 0), WK_ROW(0, 1), WK_ROW(0, 2), WK_ROW(0, 3)},
+                               {WK_ROW(1, 0), WK_ROW(1, 1), WK_ROW(1, 2), WK_ROW(1, 3)},
+                               {WK_ROW(2, 0), WK_ROW(2, 1), WK_ROW(2, 2), WK_ROW(2, 3)}};
+const InitFn kInit[3][4][2] = {{WK_IROW(0, 0), WK_IROW(0, 1), WK_IROW(0, 2), WK_IROW(0, 3)},
+                               {WK_IROW(1, 0), WK_IROW(1, 1), WK_IROW(1, 2), WK_IROW(1, 3)},
+                               {WK_IROW(2, 0), WK_IROW(2, 1), WK_IROW(2, 2), WK_IROW(2, 3)}};
 #define WK_BROW(C, S) {batch_one<C, S, false>, batch_one<C, S, true>}
-const BatchFn kBatch[3][3][2] = {{WK_BROW(0, 0), WK_BROW(0, 1), WK_BROW(0, 2)},
-                                 {WK_BROW(1, 0), WK_BROW(1, 1), WK_BROW(1, 2)},
-                                 {WK_BROW(2, 0), WK_BROW(2, 1), WK_BROW(2, 2)}};
+const BatchFn kBatch[3][4][2] = {{WK_BROW(0, 0), WK_BROW(0, 1), WK_BROW(0, 2), WK_BROW(0, 3)},
+                                 {WK_BROW(1, 0), WK_BROW(1, 1), WK_BROW(1, 2), WK_BROW(1, 3)},
+                                 {WK_BROW(2, 0), WK_BROW(2, 1), WK_BROW(2, 2), WK_BROW(2, 3)}};
 #define WK_SROW(C, S) {tiles_one<C, S, false>, tiles_one<C, S, true>}
-const TilesFn kTiles[3][3][2] = {{WK_SROW(0, 0), WK_SROW(0, 1), WK_SROW(0, 2)},
-                                 {WK_SROW(1, 0), WK_SROW(1, 1), WK_SROW(1, 2)},
-                                 {WK_SROW(2, 0), WK_SROW(2, 1), WK_SROW(2, 2)}};
+const TilesFn kTiles[3][4][2] = {{WK_SROW(0, 0), WK_SROW(0, 1), WK_SROW(0, 2), WK_SROW(0, 3)},
+                                 {WK_SROW(1, 0), WK_SROW(1, 1), WK_SROW(1, 2), WK_SROW(1, 3)},
+                                 {WK_SROW(2, 0), WK_SROW(2, 1), WK_SROW(2, 2), WK_SROW(2, 3)}};
 #undef WK_ROW
 #undef WK_IROW
 #undef WK_BROW
 #undef WK_SROW
 
-bool valid(int coll, int store) { return coll >= 0 && coll < 3 && store >= 0 && store < 3; }
+bool valid(int coll, int store) { return coll >= 0 && coll < 3 && store >= 0 && store < 4; }
 }  // namespace
 
 cudaError_t WK_CAT(launch_step_q, WK_Q)(int coll, int store, bool les, const StepArgs& a, const Launch& L,
@@ -254,21 +254,17 @@ cudaError_t WK_CAT(launch_materialise_q, WK_Q)(int store, const void* fin, const
                                               const Links& links, const Physics& phys, const Out& out,
                                               const Launch& L, int direct, const Thermal& th) {
     const int blocks = L.rows * L.xchunks;
-    if (direct) {
-        switch (store) {
-            case 0: k_direct<kQ, 0><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, phys, out, L.xchunks, th); break;
-            case 1: k_direct<kQ, 1><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, phys, out, L.xchunks, th); break;
-            case 2: k_direct<kQ, 2><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, phys, out, L.xchunks, th); break;
-            default: return cudaErrorInvalidValue;
-        }
-    } else {
-        switch (store) {
-            case 0: k_materialise<kQ, 0><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, links, phys, out, L.xchunks, th); break;
-            case 1: k_materialise<kQ, 1><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, links, phys, out, L.xchunks, th); break;
-            case 2: k_materialise<kQ, 2><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, links, phys, out, L.xchunks, th); break;
-            default: return cudaErrorInvalidValue;
-        }
+#define WK_MAT(S)                                                                               \
+    if (direct) k_direct<kQ, S><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, phys, out, L.xchunks, th); \
+    else k_materialise<kQ, S><<<blocks, L.tpb, 0, L.stream>>>(fin, flags, geo, links, phys, out, L.xchunks, th)
+    switch (store) {
+        case 0: WK_MAT(0); break;
+        case 1: WK_MAT(1); break;
+        case 2: WK_MAT(2); break;
+        case 3: WK_MAT(3); break;
+        default: return cudaErrorInvalidValue;
     }
+#undef WK_MAT
     return cudaGetLastError();
 }
 
@@ -280,25 +276,32 @@ cudaError_t launch_initial_thermal_q9(int coll, int store, bool les, const float
     const int blocks = L.rows * L.xchunks;
 #define WK_TI(C, S, LES) \
     k_initial_thermal<C, S, LES><<<blocks, L.tpb, 0, L.stream>>>(f0, t0, a, b, ta, tb, flags, geo, phys, th, L.xchunks)
-    switch (coll * 6 + store * 2 + (les ? 1 : 0)) {
+    switch (coll * 8 + store * 2 + (les ? 1 : 0)) {
         case 0: WK_TI(0, 0, false); break;
         case 1: WK_TI(0, 0, true); break;
         case 2: WK_TI(0, 1, false); break;
         case 3: WK_TI(0, 1, true); break;
         case 4: WK_TI(0, 2, false); break;
         case 5: WK_TI(0, 2, true); break;
-        case 6: WK_TI(1, 0, false); break;
-        case 7: WK_TI(1, 0, true); break;
-        case 8: WK_TI(1, 1, false); break;
-        case 9: WK_TI(1, 1, true); break;
-        case 10: WK_TI(1, 2, false); break;
-        case 11: WK_TI(1, 2, true); break;
-        case 12: WK_TI(2, 0, false); break;
-        case 13: WK_TI(2, 0, true); break;
-        case 14: WK_TI(2, 1, false); break;
-        case 15: WK_TI(2, 1, true); break;
-        case 16: WK_TI(2, 2, false); break;
-        default: WK_TI(2, 2, true); break;
+        case 6: WK_TI(0, 3, false); break;
+        case 7: WK_TI(0, 3, true); break;
+        case 8: WK_TI(1, 0, false); break;
+        case 9: WK_TI(1, 0, true); break;
+        case 10: WK_TI(1, 1, false); break;
+        case 11: WK_TI(1, 1, true); break;
+        case 12: WK_TI(1, 2, false); break;
+        case 13: WK_TI(1, 2, true); break;
+        case 14: WK_TI(1, 3, false); break;
+        case 15: WK_TI(1, 3, true); break;
+        case 16: WK_TI(2, 0, false); break;
+        case 17: WK_TI(2, 0, true); break;
+        case 18: WK_TI(2, 1, false); break;
+        case 19: WK_TI(2, 1, true); break;
+        case 20: WK_TI(2, 2, false); break;
+        case 21: WK_TI(2, 2, true); break;
+        case 22: WK_TI(2, 3, false); break;
+        case 23: WK_TI(2, 3, true); break;
+        default: return cudaErrorInvalidValue;
     }
 #undef WK_TI
     return cudaGetLastError();
@@ -322,6 +325,8 @@ cudaError_t WK_CAT(launch_rows_q, WK_Q)(int store, bool les, const StepArgs& a, 
         case 3: k_step_rows<kQ, 1, true><<<rows, tpb, 0, stream>>>(a); break;
         case 4: k_step_rows<kQ, 2, false><<<rows, tpb, 0, stream>>>(a); break;
         case 5: k_step_rows<kQ, 2, true><<<rows, tpb, 0, stream>>>(a); break;
+        case 6: k_step_rows<kQ, 3, false><<<rows, tpb, 0, stream>>>(a); break;
+        case 7: k_step_rows<kQ, 3, true><<<rows, tpb, 0, stream>>>(a); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -359,7 +364,7 @@ cudaError_t pipe_one(const StepArgs& a, const PipeArgs& p, cudaStream_t stream) 
 
 cudaError_t WK_CAT(launch_rows_pipe_q, WK_Q)(int store, bool les, int cap, const StepArgs& a, const PipeArgs& p,
                                             cudaStream_t stream) {
-    const int sel = (cap > 256 ? 6 : 0) + store * 2 + (les ? 1 : 0);
+    const int sel = (cap > 256 ? 8 : 0) + store * 2 + (les ? 1 : 0);
     switch (sel) {
         case 0: return pipe_one<0, false, 256>(a, p, stream);
         case 1: return pipe_one<0, true, 256>(a, p, stream);
@@ -367,12 +372,16 @@ cudaError_t WK_CAT(launch_rows_pipe_q, WK_Q)(int store, bool les, int cap, const
         case 3: return pipe_one<1, true, 256>(a, p, stream);
         case 4: return pipe_one<2, false, 256>(a, p, stream);
         case 5: return pipe_one<2, true, 256>(a, p, stream);
-        case 6: return pipe_one<0, false, 512>(a, p, stream);
-        case 7: return pipe_one<0, true, 512>(a, p, stream);
-        case 8: return pipe_one<1, false, 512>(a, p, stream);
-        case 9: return pipe_one<1, true, 512>(a, p, stream);
-        case 10: return pipe_one<2, false, 512>(a, p, stream);
-        case 11: return pipe_one<2, true, 512>(a, p, stream);
+        case 6: return pipe_one<3, false, 256>(a, p, stream);
+        case 7: return pipe_one<3, true, 256>(a, p, stream);
+        case 8: return pipe_one<0, false, 512>(a, p, stream);
+        case 9: return pipe_one<0, true, 512>(a, p, stream);
+        case 10: return pipe_one<1, false, 512>(a, p, stream);
+        case 11: return pipe_one<1, true, 512>(a, p, stream);
+        case 12: return pipe_one<2, false, 512>(a, p, stream);
+        case 13: return pipe_one<2, true, 512>(a, p, stream);
+        case 14: return pipe_one<3, false, 512>(a, p, stream);
+        case 15: return pipe_one<3, true, 512>(a, p, stream);
         default: return cudaErrorInvalidValue;
     }
 }

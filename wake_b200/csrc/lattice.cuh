@@ -116,10 +116,38 @@ struct Lat<27> {
 };
 
 // ---------------------------------------------------------------- storage codecs
-// STORE_F32: plain populations. STORE_F16 / STORE_BF16: the shifted,
+// STORE_F32: plain populations. STORE_F16 / STORE_BF16 / STORE_F16C: the shifted,
 // weight-normalised deviation h = f / w_q - 1, so f = w_q + w_q * h. All
 // arithmetic stays in FP32; only the HBM representation narrows.
-enum { STORE_F32 = 0, STORE_F16 = 1, STORE_BF16 = 2 };
+enum { STORE_F32 = 0, STORE_F16 = 1, STORE_BF16 = 2, STORE_F16C = 3 };
+
+// FP16C: the 16-bit float format of Lehmann et al., "On the accuracy and performance of the
+// lattice Boltzmann method with 64-bit, 32-bit, and customized 16-bit number formats",
+// Phys. Rev. E 106, 015308 (2022): 1 sign, 4 exponent and 11 mantissa bits. Here the exponent
+// field E = 1..15 encodes the binades 2^-14 .. 2^0, so a value is (-1)^s 2^(E-15) (1 + m/2^11),
+// E = 0 holds subnormals (-1)^s 2^-14 m/2^11 (steps of 2^-25), the largest magnitude is
+// 2 - 2^-11, and there is no infinity or NaN. Against IEEE half it trades the binades above 2,
+// which no stable flow's h reaches (|h| < 2 is 0 < f < 3 w), for one more significant bit.
+struct f16c_t {
+    unsigned short bits;
+};
+
+// The 15 magnitude bits placed at float32 bits 12..26 read as a float32 whose exponent field is
+// E: that float is 2^(E-127) (1 + m/2^11) (or, for E = 0, the float32 subnormal m 2^-137), and
+// the exact scaling by 2^112 makes it the FP16C value. Needs subnormal float32 arithmetic (no
+// flush to zero), which is this library's build.
+__device__ __forceinline__ float f16c_decode(unsigned b) {
+    return __uint_as_float(((b & 0x8000u) << 16) | ((b & 0x7fffu) << 12)) * 0x1p112f;
+}
+// Nearest FP16C value, ties away from zero, magnitudes above the largest saturating to it:
+// h 2^-112 is exact (or a float32 subnormal below 2^-14, finer than the format's steps), and
+// adding half a unit of bit 12 to the magnitude bits rounds it; the carry moves into the
+// exponent field where the mantissa overflows.
+__device__ __forceinline__ unsigned f16c_encode(float h) {
+    const unsigned u = __float_as_uint(__fmul_rn(h, 0x1p-112f));
+    const unsigned mag = min((u & 0x7fffffffu) + 0x800u, 0x07ffffffu);
+    return ((u >> 16) & 0x8000u) | (mag >> 12);
+}
 
 template <int S>
 struct Codec;
@@ -147,6 +175,22 @@ struct Codec<STORE_F16> {
     }
     __device__ static __forceinline__ void store_stream(T* p, float v, float w) {
         __stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(__float2half_rn(fmaf(v, 1.0f / w, -1.0f))));
+    }
+};
+
+template <>
+struct Codec<STORE_F16C> {
+    using T = f16c_t;
+    __device__ static __forceinline__ float load(const T* p, float w) {
+        return fmaf(w, f16c_decode(__ldg(reinterpret_cast<const unsigned short*>(p))), w);
+    }
+    __device__ static __forceinline__ float load_plain(const T* p, float w) { return fmaf(w, f16c_decode(p->bits), w); }
+    __device__ static __forceinline__ void store(T* p, float v, float w) {
+        p->bits = static_cast<unsigned short>(f16c_encode(fmaf(v, 1.0f / w, -1.0f)));
+    }
+    __device__ static __forceinline__ void store_stream(T* p, float v, float w) {
+        __stcs(reinterpret_cast<unsigned short*>(p),
+               static_cast<unsigned short>(f16c_encode(fmaf(v, 1.0f / w, -1.0f))));
     }
 };
 

@@ -145,6 +145,7 @@ template <int S>
 __device__ __forceinline__ float smem_one(const typename Codec<S>::T* p) {
     if constexpr (S == STORE_F32) return *p;
     else if constexpr (S == STORE_F16) return __half2float(*p);
+    else if constexpr (S == STORE_F16C) return f16c_decode(p->bits);
     else return __bfloat162float(*p);
 }
 template <int S>
@@ -154,6 +155,8 @@ __device__ __forceinline__ void smem_store_adjacent(typename Codec<S>::T* p, flo
     } else if constexpr (S == STORE_F16) {
         const __half2 h = __floats2half2_rn(v.x, v.y);
         *reinterpret_cast<__half2*>(p) = h;
+    } else if constexpr (S == STORE_F16C) {
+        *reinterpret_cast<unsigned*>(p) = f16c_encode(v.x) | (f16c_encode(v.y) << 16);
     } else {
         const __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
         *reinterpret_cast<__nv_bfloat162*>(p) = h;

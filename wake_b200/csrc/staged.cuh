@@ -140,6 +140,7 @@ template <class T>
 __device__ __forceinline__ float from_stage(T v) {
     if constexpr (std::is_same<T, float>::value) return v;
     else if constexpr (std::is_same<T, __half>::value) return __half2float(v);
+    else if constexpr (std::is_same<T, f16c_t>::value) return f16c_decode(v.bits);
     else return __bfloat162float(v);
 }
 

@@ -389,18 +389,20 @@ __device__ __forceinline__ void step_chunk(const StepArgs& a, unsigned e, int en
     }
 }
 
-// Value stored for population q: FP32 holds f, FP16 / BF16 hold h = f / w - 1.
+// Value stored for population q: FP32 holds f, FP16 / BF16 / FP16C hold h = f / w - 1.
 // load_h / store_h move the stored value itself (no decode) for the h-space math.
 template <int S>
 __device__ __forceinline__ float load_raw(const typename Codec<S>::T* p) {
     if constexpr (S == STORE_F32) return __ldg(p);
     else if constexpr (S == STORE_F16) return __half2float(__ldg(p));
+    else if constexpr (S == STORE_F16C) return f16c_decode(__ldg(reinterpret_cast<const unsigned short*>(p)));
     else return __bfloat162float(__ldg(p));
 }
 template <int S>
 __device__ __forceinline__ void store_raw(typename Codec<S>::T* p, float v) {
     if constexpr (S == STORE_F32) __stcs(p, v);
     else if constexpr (S == STORE_F16) __stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(__float2half_rn(v)));
+    else if constexpr (S == STORE_F16C) __stcs(reinterpret_cast<unsigned short*>(p), static_cast<unsigned short>(f16c_encode(v)));
     else __stcs(reinterpret_cast<unsigned short*>(p), __bfloat16_as_ushort(__float2bfloat16_rn(v)));
 }
 
@@ -409,11 +411,13 @@ __device__ __forceinline__ void store_raw(typename Codec<S>::T* p, float v) {
 template <int S>
 __device__ __forceinline__ float raw_lo(unsigned w) {
     if constexpr (S == STORE_F16) return __half2float(__ushort_as_half(static_cast<unsigned short>(w & 0xffffu)));
+    else if constexpr (S == STORE_F16C) return f16c_decode(w & 0xffffu);
     else return __bfloat162float(__ushort_as_bfloat16(static_cast<unsigned short>(w & 0xffffu)));
 }
 template <int S>
 __device__ __forceinline__ float raw_hi(unsigned w) {
     if constexpr (S == STORE_F16) return __half2float(__ushort_as_half(static_cast<unsigned short>(w >> 16)));
+    else if constexpr (S == STORE_F16C) return f16c_decode(w >> 16);
     else return __bfloat162float(__ushort_as_bfloat16(static_cast<unsigned short>(w >> 16)));
 }
 template <int S>
@@ -422,6 +426,8 @@ __device__ __forceinline__ void store_pair(typename Codec<S>::T* p, float2 v) {
     if constexpr (S == STORE_F16) {
         const __half2 h = __floats2half2_rn(v.x, v.y);  // .x in the low half
         w = *reinterpret_cast<const unsigned*>(&h);
+    } else if constexpr (S == STORE_F16C) {
+        w = f16c_encode(v.x) | (f16c_encode(v.y) << 16);
     } else {
         const __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
         w = *reinterpret_cast<const unsigned*>(&h);

@@ -20,7 +20,7 @@ from ._lib import addr, check, lib
 
 BGK, TRT, MRT = 0, 1, 2
 FLUID, SOLID, INFLOW, OUTFLOW, MOVING_WALL = 0, 1, 2, 3, 6
-STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
+STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f16c": 3}
 DEFAULT_SMAGORINSKY_CONSTANT = 0.14  # include/wake/core/constants.hpp:22
 
 
