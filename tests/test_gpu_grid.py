@@ -217,12 +217,14 @@ def test_d3q27_taylor_green_matches_oracle(collision):
 
 
 def f16c_encode_np(h):
-    """The FP16C encoder restated in numpy (float32 arithmetic with subnormals): h 2^-112, then
-    half a unit of bit 12 added to the magnitude bits (nearest, ties away from zero), magnitudes
-    from 2 - 2^-12 up saturating at 2 - 2^-11; sign in bit 15, exponent in 11..14, mantissa below."""
-    u = (np.asarray(h, np.float32) * np.float32(2.0 ** -112)).view(np.uint32)
-    mag = np.minimum((u & np.uint32(0x7FFFFFFF)) + np.uint32(0x800), np.uint32(0x07FFFFFF))
-    return (((u >> np.uint32(16)) & np.uint32(0x8000)) | (mag >> np.uint32(12))).astype(np.uint16)
+    """The FP16C encoder restated in numpy (float32 arithmetic with subnormals): the bits of
+    h 2^-112 plus half a unit of bit 12 (nearest, ties away from zero on the magnitude), then a
+    signed minimum (saturates positive values) and an unsigned one (saturates the magnitude of
+    negative values) at 2 - 2^-11; sign in bit 15, exponent in 11..14, mantissa below."""
+    u = (np.atleast_1d(np.asarray(h, np.float32)) * np.float32(2.0 ** -112)).view(np.uint32)
+    t = np.minimum((u + np.uint32(0x800)).view(np.int32), np.int32(0x07FFFFFF))
+    r = np.minimum(t.view(np.uint32), np.uint32(0x87FFFFFF))
+    return (((r >> np.uint32(12)) & np.uint32(0x7FFF)) | ((r >> np.uint32(16)) & np.uint32(0x8000))).astype(np.uint16)
 
 
 def f16c_decode_np(b):

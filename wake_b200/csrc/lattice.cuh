@@ -134,19 +134,48 @@ struct f16c_t {
 
 // The 15 magnitude bits placed at float32 bits 12..26 read as a float32 whose exponent field is
 // E: that float is 2^(E-127) (1 + m/2^11) (or, for E = 0, the float32 subnormal m 2^-137), and
-// the exact scaling by 2^112 makes it the FP16C value. Needs subnormal float32 arithmetic (no
-// flush to zero), which is this library's build.
-__device__ __forceinline__ float f16c_decode(unsigned b) {
-    return __uint_as_float(((b & 0x8000u) << 16) | ((b & 0x7fffu) << 12)) * 0x1p112f;
+// the exact scaling by 2^112 makes it the FP16C value. An arithmetic right shift by 4 of a
+// register whose top half is the value puts the magnitude there and copies the sign into bits
+// 27..31; one mask keeps bit 31. Needs subnormal float32 arithmetic (no flush to zero), which
+// is this library's build.
+__device__ __forceinline__ unsigned f16c_bits_hi(unsigned w) {  // value in bits 16..31 of w
+    return static_cast<unsigned>(static_cast<int>(w) >> 4) & 0x87fff000u;
 }
-// Nearest FP16C value, ties away from zero, magnitudes above the largest saturating to it:
-// h 2^-112 is exact (or a float32 subnormal below 2^-14, finer than the format's steps), and
-// adding half a unit of bit 12 to the magnitude bits rounds it; the carry moves into the
-// exponent field where the mantissa overflows.
+__device__ __forceinline__ unsigned f16c_bits_lo(unsigned w) {  // value in bits 0..15 of w
+    return static_cast<unsigned>(static_cast<int>(w << 16) >> 4) & 0x87ffffffu;
+}
+__device__ __forceinline__ float f16c_decode(unsigned b) { return __uint_as_float(f16c_bits_lo(b)) * 0x1p112f; }
+// .x from the high half of a, .y from the low half of b (one packed multiply)
+__device__ __forceinline__ float2 f16c_decode_hl(unsigned a, unsigned b) {
+    return __fmul2_rn(make_float2(__uint_as_float(f16c_bits_hi(a)), __uint_as_float(f16c_bits_lo(b))),
+                      make_float2(0x1p112f, 0x1p112f));
+}
+// the two values of one 32-bit word: .x the low half, .y the high half
+__device__ __forceinline__ float2 f16c_decode_word(unsigned w) {
+    return __fmul2_rn(make_float2(__uint_as_float(f16c_bits_lo(w)), __uint_as_float(f16c_bits_hi(w))),
+                      make_float2(0x1p112f, 0x1p112f));
+}
+// Nearest FP16C value, ties away from zero, magnitudes above the largest saturating to it. The
+// float32 bits of h 2^-112 (exact, or a float32 subnormal below 2^-14, finer than the format's
+// steps) plus half a unit of bit 12 round the magnitude (a mantissa carry moves into the
+// exponent field); a signed minimum then saturates positive values and an unsigned one the
+// magnitude of negative values (a NaN becomes the largest magnitude of one sign). The result
+// keeps the sign in bit 31 and the 15 field bits in 12..26.
+__device__ __forceinline__ unsigned f16c_rounded(float x_scaled) {
+    const int t = min(static_cast<int>(__float_as_uint(x_scaled) + 0x800u), 0x07ffffff);
+    return min(static_cast<unsigned>(t), 0x87ffffffu);
+}
 __device__ __forceinline__ unsigned f16c_encode(float h) {
-    const unsigned u = __float_as_uint(__fmul_rn(h, 0x1p-112f));
-    const unsigned mag = min((u & 0x7fffffffu) + 0x800u, 0x07ffffffu);
-    return ((u >> 16) & 0x8000u) | (mag >> 12);
+    const unsigned r = f16c_rounded(__fmul_rn(h, 0x1p-112f));
+    return ((r >> 12) & 0x7fffu) | ((r >> 16) & 0x8000u);
+}
+// two values to one 32-bit word (.x in the low half): one packed scaling, one byte permute
+__device__ __forceinline__ unsigned f16c_encode2(float2 v) {
+    const float2 x = __fmul2_rn(v, make_float2(0x1p-112f, 0x1p-112f));
+    const unsigned a = f16c_rounded(x.x), b = f16c_rounded(x.y);
+    const unsigned lo = ((a >> 12) & 0x7fffu) | ((a >> 16) & 0x8000u);
+    const unsigned hi = ((b << 4) & 0x7fff0000u) | (b & 0x80000000u);  // only bytes 2, 3 are taken
+    return __byte_perm(lo, hi, 0x7610);
 }
 
 template <int S>

@@ -136,10 +136,17 @@ template <int S>
 __device__ __forceinline__ float2 smem_adjacent(const typename Codec<S>::T* p) {
     if constexpr (S == STORE_F32) {
         return *reinterpret_cast<const float2*>(p);
+    } else if constexpr (S == STORE_F16C) {
+        return f16c_decode_word(*reinterpret_cast<const unsigned*>(p));
     } else {
         const unsigned w = *reinterpret_cast<const unsigned*>(p);
         return make_float2(raw_lo<S>(w), raw_hi<S>(w));
     }
+}
+// 32-bit word of a 16-bit stage row at an even element index
+template <class T>
+__device__ __forceinline__ unsigned smem_word(const T* p) {
+    return *reinterpret_cast<const unsigned*>(p);
 }
 template <int S>
 __device__ __forceinline__ float smem_one(const typename Codec<S>::T* p) {
@@ -156,7 +163,7 @@ __device__ __forceinline__ void smem_store_adjacent(typename Codec<S>::T* p, flo
         const __half2 h = __floats2half2_rn(v.x, v.y);
         *reinterpret_cast<__half2*>(p) = h;
     } else if constexpr (S == STORE_F16C) {
-        *reinterpret_cast<unsigned*>(p) = f16c_encode(v.x) | (f16c_encode(v.y) << 16);
+        *reinterpret_cast<unsigned*>(p) = f16c_encode2(v);
     } else {
         const __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
         *reinterpret_cast<__nv_bfloat162*>(p) = h;
@@ -262,9 +269,18 @@ __global__ void __launch_bounds__(CAP / 2 + 32, CAP > 256 ? 1 : (S == STORE_F32 
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
                 const T* r = st + q * CAP;
-                if (L::cx(q) == 0) f[q] = smem_adjacent<S>(r + xa);
-                else if (L::cx(q) > 0) f[q] = make_float2(smem_one<S>(r + xm), smem_one<S>(r + xa));
-                else f[q] = make_float2(smem_one<S>(r + xa + 1), smem_one<S>(r + xp));
+                if (L::cx(q) == 0) {
+                    f[q] = smem_adjacent<S>(r + xa);
+                } else if constexpr (S == STORE_F16C) {
+                    // the shifted pair from two aligned words: the high half of one, the low half
+                    // of the next (xm - 1, xa, xp even)
+                    f[q] = L::cx(q) > 0 ? f16c_decode_hl(smem_word(r + (xm - 1)), smem_word(r + xa))
+                                        : f16c_decode_hl(smem_word(r + xa), smem_word(r + xp));
+                } else if (L::cx(q) > 0) {
+                    f[q] = make_float2(smem_one<S>(r + xm), smem_one<S>(r + xa));
+                } else {
+                    f[q] = make_float2(smem_one<S>(r + xa + 1), smem_one<S>(r + xp));
+                }
             }
             if ((kind & ROW_ZH_IN) && xa == 0) zou_he_half<Q, HS>(f, 0, FL_ZH_IN, a.geo);
             if ((kind & ROW_ZH_OUT) && xa + 2 == nx) zou_he_half<Q, HS>(f, 1, FL_ZH_OUT, a.geo);

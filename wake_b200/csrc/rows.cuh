@@ -37,6 +37,8 @@ template <int S>
 __device__ __forceinline__ float2 load_adjacent(const typename Codec<S>::T* p) {
     if constexpr (S == STORE_F32) {
         return __ldg(reinterpret_cast<const float2*>(p));
+    } else if constexpr (S == STORE_F16C) {
+        return f16c_decode_word(__ldg(reinterpret_cast<const unsigned*>(p)));
     } else {
         const unsigned w = __ldg(reinterpret_cast<const unsigned*>(p));
         return make_float2(raw_lo<S>(w), raw_hi<S>(w));

@@ -427,7 +427,7 @@ __device__ __forceinline__ void store_pair(typename Codec<S>::T* p, float2 v) {
         const __half2 h = __floats2half2_rn(v.x, v.y);  // .x in the low half
         w = *reinterpret_cast<const unsigned*>(&h);
     } else if constexpr (S == STORE_F16C) {
-        w = f16c_encode(v.x) | (f16c_encode(v.y) << 16);
+        w = f16c_encode2(v);
     } else {
         const __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
         w = *reinterpret_cast<const unsigned*>(&h);
