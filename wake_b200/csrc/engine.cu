@@ -429,8 +429,9 @@ int rebuild_flags(wake_grid* g) {
         std::vector<uint8_t> row_fast(static_cast<std::size_t>(g->rows), 1);
         for (long long e = 0; e < nsegs; ++e) {
             if (h[e] & 1) continue;
-            gen.push_back(static_cast<unsigned>(e));
             row_fast[static_cast<std::size_t>(e / nseg)] = 0;
+            if (h[e] & 4) continue;  // every node solid: frozen in both buffers, nothing to launch
+            gen.push_back(static_cast<unsigned>(e));
         }
         for (int r = 0; r < g->rows; ++r) {
             if (row_fast[r]) {

@@ -78,7 +78,7 @@ __global__ void k_flags(const uint8_t* __restrict__ types, uint8_t* __restrict__
 
 // Segment classes for the two step kernels (one warp per segment of SEG nodes):
 // bit 0 = every node is a pure gather (k_step_fast), bit 1 = the segment holds
-// a momentum-exchange node.
+// a momentum-exchange node, bit 2 = every node is solid (no launch needed).
 template <int Q>
 __global__ void k_seg_class(const uint8_t* __restrict__ flags, uint8_t* __restrict__ cls, const Geo geo,
                             long long nsegs) {
@@ -86,15 +86,17 @@ __global__ void k_seg_class(const uint8_t* __restrict__ flags, uint8_t* __restri
     if (e >= nsegs) return;
     const Seg sg = seg_decode(static_cast<unsigned>(e), geo);
     const int lane = threadIdx.x & 31;
-    int fast = 1, mem = 0;
+    int fast = 1, mem = 0, solid = 1;
     for (int x = sg.x0 + lane; x < sg.x1; x += 32) {
         const uint8_t fl = flags[sg.row0 + x];
         fast &= (fl & FL_FAST) ? 1 : 0;
         mem |= (fl & FL_MEM) ? 1 : 0;
+        solid &= (fl & FL_TYPE) == CT_SOLID ? 1 : 0;
     }
     fast = __all_sync(0xffffffffu, fast);
     mem = __any_sync(0xffffffffu, mem);
-    if (lane == 0) cls[e] = static_cast<uint8_t>((fast ? 1 : 0) | (mem ? 2 : 0));
+    solid = __all_sync(0xffffffffu, solid);
+    if (lane == 0) cls[e] = static_cast<uint8_t>((fast ? 1 : 0) | (mem ? 2 : 0) | (solid ? 4 : 0));
 }
 
 // Pull-free read of f^0 (state buffer holding pre-collision populations).
