@@ -149,7 +149,7 @@ void step_one(const StepArgs& a, const Launch& L, bool fast) {
         else k_step_fast<kQ, C, S, LES, false><<<a.nspans, L.tpb_fast, 0, L.stream>>>(a);
     } else {
         if (a.nrows <= 0) return;
-        k_step<kQ, C, S, LES><<<a.nrows, 64, 0, L.stream>>>(a);
+        k_step<kQ, C, S, LES><<<a.nrows, SEG, 0, L.stream>>>(a);
     }
 }
 template <int C, int S, bool LES>
@@ -165,7 +165,7 @@ void batch_one(const BatchArgs& b, int tpb, cudaStream_t st, bool fast, bool idx
         else k_step_fast_batch<kQ, C, S, LES, false><<<b.nspans, tpb, 0, st>>>(b);
     } else {
         if (b.nrows <= 0) return;
-        k_step_batch<kQ, C, S, LES><<<b.nrows, 64, 0, st>>>(b);
+        k_step_batch<kQ, C, S, LES><<<b.nrows, SEG, 0, st>>>(b);
     }
 }
 // Persistent tile kernel: TILE_CTAS_PER_SM CTAs per SM (capped by the work), dynamic shared

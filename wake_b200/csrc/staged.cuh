@@ -237,9 +237,10 @@ __global__ void __launch_bounds__(TILE_THREADS, TILE_CTAS_PER_SM) k_step_tiles(c
     // 32-node chunk, pure-gather spans one CTA per span (the direct kernels' paths)
     {
         const int warps = blockDim.x >> 5;
-        for (int g = first * warps + static_cast<int>(threadIdx.x >> 5); g < 2 * t.ngen; g += stride * warps) {
-            const uint4 r = t.gen[g >> 1];
-            step_chunk<Q, COLL, S, LES>(tile_member<BATCH>(a0, t, r.x), r.y, static_cast<int>(r.z), g & 1);
+        constexpr int CPS = SEG / 32;  // warp chunks per segment
+        for (int g = first * warps + static_cast<int>(threadIdx.x >> 5); g < CPS * t.ngen; g += stride * warps) {
+            const uint4 r = t.gen[g / CPS];
+            step_chunk<Q, COLL, S, LES>(tile_member<BATCH>(a0, t, r.x), r.y, static_cast<int>(r.z), g % CPS);
         }
         for (int sp = first; sp < t.nspans; sp += stride) {
             const uint4 r = t.spans[sp];

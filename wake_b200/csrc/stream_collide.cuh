@@ -290,8 +290,13 @@ struct StepArgs {
 // Work unit of the step kernels: a segment of up to SEG consecutive nodes of one
 // row, numbered row * nseg + s with nseg = ceil(nx / SEG) and row = z * ny + y.
 // Rows are split so that only the segments next to a wall, obstacle or curved
-// link take the general per-node path.
-constexpr int SEG = 64;
+// link take the general per-node path. The general kernels run one warp per
+// 32-node chunk of a segment.
+#ifndef WK_SEG
+#define WK_SEG 64
+#endif
+constexpr int SEG = WK_SEG;
+static_assert(SEG == 32 || SEG == 64, "segments of one or two warp chunks");
 
 struct Seg {
     int y, z, x0, x1;
@@ -661,7 +666,7 @@ __device__ __forceinline__ void step_span_fast(const StepArgs& a, const Seg& sg)
     }
 }
 
-// Single lattice. General segments: one 64-thread block per segment (a warp per
+// Single lattice. General segments: one SEG-thread block per segment (a warp per
 // 32-node chunk). Pure-gather spans: one block per span.
 template <int Q, int COLL, int S, bool LES>
 __global__ void __launch_bounds__(64) k_step(const StepArgs a) {
