@@ -17,14 +17,15 @@
 // once the compute threads mark a row's results in place (mbarrier `written`) it
 // stores that row and, when the stores have read the stage, loads the row NS further
 // on into it. CAP / 2 compute threads (one adjacent node pair each) wait for a stage's
-// inputs (mbarrier `full`), compute, and meet at a named barrier before writing the
-// results in place, so no CTA-wide barrier stalls the copies. Several CTAs per SM
-// interleave their phases.
+// inputs (mbarrier `full`), compute, and meet at one named barrier per row before
+// writing the results in place, so no CTA-wide barrier stalls the copies. Several
+// CTAs per SM interleave their phases.
 //
 // Every wait is bounded: a stage that does not arrive within ~2^22 polls sets
-// ERR_STAGE_TIMEOUT in the lattice's status word; the compute threads leave
-// together (a reducing named barrier), the producer gives up on its next bounded
-// wait, drains its stores and gives loads in flight a bounded chance to land.
+// ERR_STAGE_TIMEOUT in the lattice's status word; the compute threads skip the
+// row's arithmetic and leave together at the row's named barrier (it ANDs their
+// wait results; nothing is written back), the producer gives up on its next
+// bounded wait, drains its stores and gives loads in flight a bounded chance to land.
 //
 // Requirements (host-checked): TRT; nx even, nx <= CAP, nx * sizeof(T) a multiple
 // of 16 bytes (bulk copies move whole 16-byte units from 16-byte-aligned
@@ -259,13 +260,9 @@ __global__ void __launch_bounds__(CAP / 2 + 32, CAP > 256 ? 1 : (S == STORE_F32 
         const int s = it % NS;
         const unsigned kind = p.rows[first + it * stride] >> 28;
         const bool ok = mbar_wait(smem_addr(&full[s]), static_cast<unsigned>((it / NS) & 1));
-        if (!compute_bar_and(ok, NC)) {
-            if (threadIdx.x == 0) atomicOr(a.status, ERR_STAGE_TIMEOUT);
-            break;
-        }
         T* st = reinterpret_cast<T*>(stages + s * STAGE_B);
         float2 f[Q];
-        if (live) {
+        if (live && ok) {
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
                 const T* r = st + q * CAP;
@@ -289,7 +286,12 @@ __global__ void __launch_bounds__(CAP / 2 + 32, CAP > 256 ? 1 : (S == STORE_F32 
             if (!(rho.x > 0.0f) || !(fabsf(u[0].x) < 1e30f) || !(rho.y > 0.0f) || !(fabsf(u[0].y) < 1e30f))
                 atomicOr(a.status, ERR_NONFINITE);
         }
-        (void)compute_bar_and(true, NC);  // every input of the stage has been read
+        // one barrier per row: every input of the stage has been read (the results go back in
+        // place), and a wait that ran out anywhere ends the loop for every compute thread
+        if (!compute_bar_and(ok, NC)) {
+            if (threadIdx.x == 0) atomicOr(a.status, ERR_STAGE_TIMEOUT);
+            break;
+        }
         if (live) {
 #pragma unroll
             for (int q = 0; q < Q; ++q) smem_store_adjacent<S>(st + q * CAP + xa, f[q]);
